@@ -1,0 +1,154 @@
+/*
+ * libaccint-b200: C ABI of the B200-native two-electron J/K engine.
+ *
+ * Rys-quadrature electron-repulsion integrals over contracted Cartesian
+ * Gaussians (l <= 4), Schwarz-screened, digested straight into Coulomb (J) and
+ * exchange (K) matrices on one NVIDIA B200 (sm_100a).  Plain C types only: every
+ * matrix is a row-major nbf x nbf array of doubles, every pointer is owned by the
+ * caller, and every function returns 0 (LAI_OK) or a negative error code; no C++
+ * exception crosses this boundary.  lai_last_error() gives a message for the
+ * calling thread.  An engine is not thread-safe: serialize calls per engine
+ * (the reference's FockBuilder has the same contract,
+ * include/libaccint/consumers/fock_builder.hpp).
+ *
+ * Basis conventions are the reference's (LibAccInt v0.1.0-alpha.2):
+ *   - Cartesian components ordered lx descending, then ly descending
+ *     (include/libaccint/math/cartesian_indices.hpp:26-36);
+ *   - contraction coefficients normalized so the (l,0,0) component has unit
+ *     self-overlap, each component scaled by 1/sqrt((2lx-1)!!(2ly-1)!!(2lz-1)!!)
+ *     (src/shared/basis/shell.cpp:32-113, include/libaccint/kernels/norm_correction.hpp:28-34);
+ *   - basis functions numbered shell by shell in input order
+ *     (src/shared/basis/basis_set.cpp:161-185);
+ *   - J_mn = sum_ls (mn|ls) D_ls, K_ml = sum_ns (mn|ls) D_ns
+ *     (include/libaccint/consumers/fock_builder.hpp:41-43).
+ */
+#ifndef LIBACCINT_B200_H
+#define LIBACCINT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LAI_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LAI_API __attribute__((visibility("default")))
+#else
+#define LAI_API
+#endif
+
+enum lai_status {
+  LAI_OK = 0,
+  LAI_EINVAL = -1,   /* bad argument (sizes, null pointers, l > 4, ...)      */
+  LAI_ENOMEM = -2,   /* device or host allocation failed                      */
+  LAI_ECUDA = -3,    /* CUDA runtime error (no device, launch failure, ...)   */
+  LAI_ETIMEOUT = -4, /* a bounded device wait gave up                         */
+  LAI_ESTATE = -5,   /* call out of order (e.g. no density set)               */
+  LAI_ENOTSUP = -6   /* feature not available in this build                   */
+};
+
+typedef struct lai_basis lai_basis;
+typedef struct lai_engine lai_engine;
+
+/* Last error message of the calling thread (never NULL). */
+LAI_API const char* lai_last_error(void);
+LAI_API int lai_abi_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Basis.  Replaces Shell(am, center, exps, coefs) + BasisSet(shells)
+ * (src/shared/basis/shell.cpp:163-187, src/shared/basis/basis_set.cpp:21-29).
+ * l[s], nprim[s]: angular momentum (0..4) and primitive count of shell s;
+ * centers[3*s..]: Bohr; exps/coefs: primitives of all shells concatenated.
+ * Coefficients are RAW contraction coefficients and are normalized here exactly
+ * like the reference Shell constructor, unless flags has LAI_BASIS_PRENORMALIZED.
+ * atom_index may be NULL (then every shell gets its own atom id = -1).
+ * ------------------------------------------------------------------------- */
+#define LAI_BASIS_PRENORMALIZED 1
+LAI_API int lai_basis_create(int nshell, const int* l, const int* nprim, const double* centers,
+                     const double* exps, const double* coefs, const int* atom_index, int flags,
+                     lai_basis** out);
+LAI_API void lai_basis_destroy(lai_basis* basis);
+LAI_API long lai_basis_nbf(const lai_basis* basis);
+LAI_API int lai_basis_nshell(const lai_basis* basis);
+/* Shell s after normalization: exps/coefs get nprim entries (input order, zero
+ * coefficients kept); func_index = first basis function of the shell. */
+LAI_API int lai_basis_shell(const lai_basis* basis, int s, int* l, int* nprim, double* center,
+                    double* exps, double* coefs, long* func_index);
+
+/* ---------------------------------------------------------------------------
+ * Engine: device-resident pair data for one basis, Schwarz bounds and the
+ * sorted pair lists.  Replaces Engine(basis) + precompute_schwarz_bounds()
+ * (include/libaccint/engine/engine.hpp:86-107,1578-1583).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  double schwarz_threshold; /* pass iff Q_ij*Q_kl >= threshold (default 1e-12) */
+  int device;               /* CUDA device ordinal (default 0)                  */
+} lai_engine_opts;
+LAI_API void lai_engine_opts_default(lai_engine_opts* opts);
+LAI_API int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_engine** out);
+LAI_API void lai_engine_destroy(lai_engine* engine);
+/* Schwarz bounds Q[i*nshell+j] = sqrt(max |(ij|ij)|) of all shell pairs
+ * (src/shared/screening/schwarz_bounds.cpp:20-59). */
+LAI_API int lai_engine_schwarz(lai_engine* engine, double* Q);
+
+/* ---------------------------------------------------------------------------
+ * J/K build.  Replaces Engine::compute(Operator::coulomb(), FockBuilder&) and
+ * Engine::compute_and_consume(op, FockBuilder&, ScreeningOptions)
+ * (include/libaccint/engine/engine.hpp:435-499,727-731,1635-1666) followed by
+ * FockBuilder::get_coulomb_matrix()/get_exchange_matrix()
+ * (include/libaccint/consumers/fock_builder.hpp:111-119).
+ * D must be symmetric (the reference's symmetric scatter assumes it too,
+ * src/shared/consumers/fock_builder.cpp:163-171).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  double fp32_cut;   /* mixed precision: quartets with Q_ij*Q_kl*max|D| < fp32_cut
+                        run the Rys recursion in FP32 (0 = all FP64)             */
+  int check_symmetric; /* 1 = reject a D that is not symmetric to 1e-12 (host)  */
+} lai_jk_opts;
+LAI_API void lai_jk_opts_default(lai_jk_opts* opts);
+
+typedef struct {
+  int64_t quartets_fp64;   /* canonical shell quartets computed in FP64       */
+  int64_t quartets_fp32;   /* ... and in FP32                                 */
+  double alg_flops;        /* algorithmic FP work of those quartets (FLOP)    */
+  double seconds_device;   /* device time of the integral + digestion kernels */
+  double seconds_total;    /* wall time of the call                           */
+  int kernel_launches;     /* kernels launched by the call                    */
+} lai_jk_report;
+
+/* Host buffers (nbf*nbf doubles each). report may be NULL. */
+LAI_API int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double* J, double* K,
+                 const lai_jk_opts* opts, lai_jk_report* report);
+/* Device buffers on the engine's device; stream is a cudaStream_t (NULL = legacy
+ * default stream).  Asynchronous: returns after enqueueing (report times are
+ * then not filled). */
+LAI_API int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d_J, double* d_K,
+                        void* stream, const lai_jk_opts* opts, lai_jk_report* report);
+
+/* ---------------------------------------------------------------------------
+ * Raw integrals of every canonical shell quartet that passes the engine's
+ * Schwarz threshold.  Replaces Engine::compute_batch_screened(op, screening)
+ * (include/libaccint/engine/engine.hpp:1181-1187) returning IntegralBuffers with
+ * quartet_meta {offset, fi..fl, na..nd} (include/libaccint/engine/integral_buffer.hpp:27-35).
+ * Each quartet's block is [a][b][c][d] row-major starting at meta.offset, in the
+ * shell order given by the function offsets fa..fd (one representative of the
+ * 8-fold permutation orbit; all quartets are distinct orbits).
+ * Call with out == NULL / meta == NULL to get the counts only.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int64_t offset;
+  int32_t fa, fb, fc, fd;
+  int32_t na, nb, nc, nd;
+} lai_quartet_meta;
+LAI_API int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_capacity,
+                                   lai_quartet_meta* meta, size_t meta_capacity,
+                                   int64_t* n_quartets, int64_t* n_values);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIBACCINT_B200_H */

@@ -1,0 +1,9 @@
+"""libaccint-b200: B200-native Rys-quadrature two-electron J/K engine.
+
+Import with ``importlib.import_module("libaccint-public_b200")`` (the package
+directory name is not a Python identifier).
+"""
+from ._lib import LibAccIntError, lib  # noqa: F401
+from .basis import BasisSet, Shell, basis_data  # noqa: F401
+from .engine import Engine, FockBuilder, Operator, ScreeningOptions, jk  # noqa: F401
+from . import molecules, workloads  # noqa: F401

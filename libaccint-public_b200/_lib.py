@@ -1,0 +1,92 @@
+"""ctypes binding of the C ABI declared in include/libaccint_b200.h.
+
+The library is the in-tree ``libaccint_b200.so`` built by ``build.py``.  There is
+no fallback: if the library is missing or a CUDA device is absent, calls fail
+loudly with ``LibAccIntError``.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaccint_b200.so")
+
+LAI_OK, LAI_EINVAL, LAI_ENOMEM, LAI_ECUDA, LAI_ETIMEOUT, LAI_ESTATE, LAI_ENOTSUP = 0, -1, -2, -3, -4, -5, -6
+LAI_BASIS_PRENORMALIZED = 1
+
+# Every symbol include/libaccint_b200.h declares (checked by the CPU test suite).
+EXPORTED = [
+    "lai_last_error", "lai_abi_version",
+    "lai_basis_create", "lai_basis_destroy", "lai_basis_nbf", "lai_basis_nshell", "lai_basis_shell",
+    "lai_engine_opts_default", "lai_engine_create", "lai_engine_destroy", "lai_engine_schwarz",
+    "lai_jk_opts_default", "lai_jk_build", "lai_jk_build_device", "lai_eri_batch_screened",
+]
+
+
+class LibAccIntError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libaccint_b200 error {code}: {msg}")
+        self.code = code
+
+
+class EngineOpts(ctypes.Structure):
+    _fields_ = [("schwarz_threshold", ctypes.c_double), ("device", ctypes.c_int)]
+
+
+class JKOpts(ctypes.Structure):
+    _fields_ = [("fp32_cut", ctypes.c_double), ("check_symmetric", ctypes.c_int)]
+
+
+class QuartetMeta(ctypes.Structure):
+    _fields_ = [("offset", ctypes.c_int64), ("fa", ctypes.c_int32), ("fb", ctypes.c_int32),
+                ("fc", ctypes.c_int32), ("fd", ctypes.c_int32), ("na", ctypes.c_int32),
+                ("nb", ctypes.c_int32), ("nc", ctypes.c_int32), ("nd", ctypes.c_int32)]
+
+
+class JKReport(ctypes.Structure):
+    _fields_ = [("quartets_fp64", ctypes.c_int64), ("quartets_fp32", ctypes.c_int64),
+                ("alg_flops", ctypes.c_double), ("seconds_device", ctypes.c_double),
+                ("seconds_total", ctypes.c_double), ("kernel_launches", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the shared library once (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise LibAccIntError(LAI_ENOTSUP, f"{LIB_PATH} not built (run build.py)")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, D, V, L64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, None, ctypes.c_long
+    sig = {
+        "lai_last_error": (ctypes.c_char_p, []),
+        "lai_abi_version": (I, []),
+        "lai_basis_create": (I, [I, P, P, P, P, P, P, I, ctypes.POINTER(P)]),
+        "lai_basis_destroy": (V, [P]),
+        "lai_basis_nbf": (L64, [P]),
+        "lai_basis_nshell": (I, [P]),
+        "lai_basis_shell": (I, [P, I, P, P, P, P, P, P]),
+        "lai_engine_opts_default": (V, [ctypes.POINTER(EngineOpts)]),
+        "lai_engine_create": (I, [P, ctypes.POINTER(EngineOpts), ctypes.POINTER(P)]),
+        "lai_engine_destroy": (V, [P]),
+        "lai_engine_schwarz": (I, [P, P]),
+        "lai_jk_opts_default": (V, [ctypes.POINTER(JKOpts)]),
+        "lai_jk_build": (I, [P, P, ctypes.c_size_t, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKReport)]),
+        "lai_jk_build_device": (I, [P, P, P, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKReport)]),
+        "lai_eri_batch_screened": (I, [P, P, ctypes.c_size_t, P, ctypes.c_size_t,
+                                       ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != LAI_OK:
+        raise LibAccIntError(rc, lib().lai_last_error().decode())
+    return rc

@@ -1,0 +1,133 @@
+"""Basis sets: shells of contracted Cartesian Gaussians on atoms.
+
+Mirrors the reference's ``Shell`` / ``BasisSet`` (include/libaccint/basis/shell.hpp,
+src/shared/basis/basis_set.cpp): shells are emitted per atom in the order of the
+basis-set data (the BSE reader's order, src/shared/data/bse_json_parser.cpp:27-87),
+functions are numbered shell by shell, and contraction coefficients are given raw
+and normalized by the library exactly like the reference Shell constructor.
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+
+from . import _lib
+
+_DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "basis_sets.json")
+_SYMBOL = {1: "H", 6: "C", 7: "N", 8: "O"}
+_cache = None
+
+
+def basis_data(name):
+    """Per-element shell lists [(l, exps, coefs), ...] of a bundled basis set."""
+    global _cache
+    if _cache is None:
+        with open(_DATA) as f:
+            _cache = json.load(f)["basis_sets"]
+    key = name.lower()
+    if key in ("sto-3g", "sto3g"):
+        key = "sto-3g-builtin"  # the reference's create_builtin_basis("sto-3g") data
+    if key not in _cache:
+        raise KeyError(f"basis set {name!r} not bundled (have {sorted(_cache)})")
+    return _cache[key]
+
+
+class Shell:
+    __slots__ = ("l", "center", "exps", "coefs", "atom")
+
+    def __init__(self, l, center, exps, coefs, atom=-1):
+        self.l = int(l)
+        self.center = np.asarray(center, dtype=np.float64).reshape(3)
+        self.exps = np.asarray(exps, dtype=np.float64)
+        self.coefs = np.asarray(coefs, dtype=np.float64)
+        self.atom = int(atom)
+
+    @property
+    def n_functions(self):
+        return (self.l + 1) * (self.l + 2) // 2
+
+
+class BasisSet:
+    """A list of shells plus the C-ABI handle (created lazily)."""
+
+    def __init__(self, shells, prenormalized=False):
+        self.shells = list(shells)
+        self.prenormalized = prenormalized
+        self._handle = None
+
+    @classmethod
+    def from_atoms(cls, Z, xyz, name):
+        data = basis_data(name)
+        shells = []
+        xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
+        for a, (z, r) in enumerate(zip(Z, xyz)):
+            sym = _SYMBOL.get(int(z))
+            if sym is None or sym not in data:
+                raise KeyError(f"element Z={z} not in basis {name}")
+            for l, e, c in data[sym]:
+                shells.append(Shell(l, r, e, c, a))
+        return cls(shells)
+
+    # --- flat arrays (the C-ABI layout) ---
+    def arrays(self):
+        l = np.array([s.l for s in self.shells], dtype=np.int32)
+        nprim = np.array([len(s.exps) for s in self.shells], dtype=np.int32)
+        centers = np.array([s.center for s in self.shells], dtype=np.float64).reshape(-1)
+        exps = np.concatenate([s.exps for s in self.shells]) if self.shells else np.zeros(0)
+        coefs = np.concatenate([s.coefs for s in self.shells]) if self.shells else np.zeros(0)
+        atom = np.array([s.atom for s in self.shells], dtype=np.int32)
+        return l, nprim, centers, np.ascontiguousarray(exps), np.ascontiguousarray(coefs), atom
+
+    @property
+    def n_shells(self):
+        return len(self.shells)
+
+    @property
+    def nbf(self):
+        return sum(s.n_functions for s in self.shells)
+
+    @property
+    def max_l(self):
+        return max(s.l for s in self.shells)
+
+    def function_offsets(self):
+        off = np.zeros(len(self.shells) + 1, dtype=np.int64)
+        for i, s in enumerate(self.shells):
+            off[i + 1] = off[i] + s.n_functions
+        return off
+
+    def handle(self):
+        if self._handle is None:
+            L = _lib.lib()
+            l, nprim, centers, exps, coefs, atom = self.arrays()
+            self._arrs = (l, nprim, centers, exps, coefs, atom)
+            h = ctypes.c_void_p()
+            _lib.check(L.lai_basis_create(len(self.shells), l.ctypes.data, nprim.ctypes.data,
+                                          centers.ctypes.data, exps.ctypes.data, coefs.ctypes.data,
+                                          atom.ctypes.data,
+                                          _lib.LAI_BASIS_PRENORMALIZED if self.prenormalized else 0,
+                                          ctypes.byref(h)))
+            self._handle = h
+        return self._handle
+
+    def normalized_coefs(self):
+        """Normalized coefficients per shell as computed by the library."""
+        L = _lib.lib()
+        out = []
+        for i, s in enumerate(self.shells):
+            e = np.zeros(len(s.exps))
+            c = np.zeros(len(s.exps))
+            li = ctypes.c_int()
+            np_ = ctypes.c_int()
+            ctr = np.zeros(3)
+            fi = ctypes.c_long()
+            _lib.check(L.lai_basis_shell(self.handle(), i, ctypes.byref(li), ctypes.byref(np_),
+                                         ctr.ctypes.data, e.ctypes.data, c.ctypes.data, ctypes.byref(fi)))
+            out.append(c)
+        return out
+
+    def __del__(self):
+        if getattr(self, "_handle", None) is not None and _lib._lib is not None:
+            _lib._lib.lai_basis_destroy(self._handle)
+            self._handle = None

@@ -1,0 +1,723 @@
+// Host orchestration of the J/K engine and the C ABI (include/libaccint_b200.h).
+//
+// Pipeline of one engine (built once per basis, reused for every density):
+//   1. lai_basis_create: normalize contraction coefficients like the reference
+//      Shell constructor (src/shared/basis/shell.cpp:32-113); drop primitives whose
+//      normalized coefficient is exactly zero (general-contraction padding kept by
+//      the reference's BSE reader, src/shared/data/bse_json_parser.cpp:43-57 --
+//      their contribution is exactly zero).
+//   2. Shell pairs (i >= j) oriented so la >= lb, grouped into pair classes
+//      (la, lb, Ka, Kb); primitive-pair data (zeta, P, P-A, prefactor) in SoA.
+//   3. Schwarz bounds from the diagonal quartets (ab|ab) on the device
+//      (src/shared/screening/schwarz_bounds.cpp:20-59 computes the same on the host).
+//   4. Pairs sorted by Q (descending) within their class; pairs with
+//      Q * Q_max < threshold dropped; for every ordered class pair (bra >= ket) the
+//      number of passing kets of each bra pair is a prefix length (binary search),
+//      prefix-summed into the launch's flat quartet range.
+//   5. lai_jk_build: one launch per class pair (thread-per-quartet kernels for the
+//      small classes, warp-per-quartet otherwise), then J = J' + J'^T, K = K' + K'^T.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/libaccint_b200.h"
+#include "eri_kernels.h"
+#include "rys_tables.inc"
+
+static_assert(RYS_DEG == lai::kRysDeg, "table degree mismatch");
+static_assert(BOYS_NM == lai::kBoysNM, "Boys table width mismatch");
+static_assert(BOYS_NGRID == lai::kBoysNGrid, "Boys grid mismatch");
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define LAI_CUDA_TRY(expr)                                                              \
+  do {                                                                                  \
+    cudaError_t e_ = (expr);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(e_ == cudaErrorMemoryAllocation ? LAI_ENOMEM : LAI_ECUDA,             \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                  \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t alloc(size_t n) {
+    if (p) { cudaFree(p); p = nullptr; }
+    bytes = n;
+    if (n == 0) return cudaSuccess;
+    return cudaMalloc(&p, n);
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+template <typename T>
+cudaError_t upload(DevBuf& b, const std::vector<T>& v) {
+  cudaError_t e = b.alloc(v.size() * sizeof(T));
+  if (e != cudaSuccess || v.empty()) return e;
+  return cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+double dfact_odd(int l) {
+  double r = 1;
+  for (int k = 2 * l - 1; k > 1; k -= 2) r *= k;
+  return r;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Basis
+// ---------------------------------------------------------------------------
+struct HostShell {
+  int l;
+  double center[3];
+  std::vector<double> exps_all, coefs_all;  // normalized, all primitives as given
+  std::vector<double> exps, coefs;          // nonzero-coefficient primitives only
+  int atom;
+  long func;
+};
+
+struct lai_basis {
+  std::vector<HostShell> shells;
+  long nbf = 0;
+};
+
+extern "C" {
+
+const char* lai_last_error(void) { return g_last_error.c_str(); }
+int lai_abi_version(void) { return LAI_ABI_VERSION; }
+
+int lai_basis_create(int nshell, const int* l, const int* nprim, const double* centers,
+                     const double* exps, const double* coefs, const int* atom_index, int flags,
+                     lai_basis** out) {
+  if (!out) return fail(LAI_EINVAL, "lai_basis_create: out is NULL");
+  *out = nullptr;
+  if (nshell < 0 || (nshell > 0 && (!l || !nprim || !centers || !exps || !coefs)))
+    return fail(LAI_EINVAL, "lai_basis_create: null array");
+  auto b = std::make_unique<lai_basis>();
+  long off = 0;
+  for (int s = 0; s < nshell; ++s) {
+    if (l[s] < 0 || l[s] > lai::kMaxL)
+      return fail(LAI_EINVAL, "lai_basis_create: shell " + std::to_string(s) +
+                                  " angular momentum outside [0, 4]");
+    if (nprim[s] < 1) return fail(LAI_EINVAL, "lai_basis_create: shell with no primitive");
+    HostShell sh;
+    sh.l = l[s];
+    for (int x = 0; x < 3; ++x) sh.center[x] = centers[3 * s + x];
+    sh.atom = atom_index ? atom_index[s] : -1;
+    sh.exps_all.assign(exps + off, exps + off + nprim[s]);
+    sh.coefs_all.assign(coefs + off, coefs + off + nprim[s]);
+    off += nprim[s];
+    for (double e : sh.exps_all)
+      if (!(e > 0.0)) return fail(LAI_EINVAL, "lai_basis_create: non-positive exponent");
+    if (!(flags & LAI_BASIS_PRENORMALIZED)) {
+      // Reference Shell normalization (shell.cpp:32-113): primitive factor
+      // (2a/pi)^{3/4} (4a)^{l/2} / sqrt((2l-1)!!), then unit (l,0,0) self-overlap.
+      const int L = sh.l;
+      const int n = (int)sh.exps_all.size();
+      for (int p = 0; p < n; ++p) {
+        const double a = sh.exps_all[p];
+        sh.coefs_all[p] *= std::pow(2.0 * a / M_PI, 0.75) * std::pow(4.0 * a, 0.5 * L) /
+                           std::sqrt(dfact_odd(L));
+      }
+      double ov = 0.0;
+      for (int p = 0; p < n; ++p)
+        for (int q = 0; q < n; ++q) {
+          const double z = sh.exps_all[p] + sh.exps_all[q];
+          double o = std::pow(M_PI / z, 1.5);
+          for (int k = 0; k < L; ++k) o *= 0.5 / z;
+          ov += sh.coefs_all[p] * sh.coefs_all[q] * o;
+        }
+      if (!(ov > 0.0)) return fail(LAI_EINVAL, "lai_basis_create: zero contraction");
+      const double sc = 1.0 / std::sqrt(ov);
+      for (auto& c : sh.coefs_all) c *= sc;
+    }
+    for (size_t p = 0; p < sh.exps_all.size(); ++p)
+      if (sh.coefs_all[p] != 0.0) {
+        sh.exps.push_back(sh.exps_all[p]);
+        sh.coefs.push_back(sh.coefs_all[p]);
+      }
+    if (sh.exps.empty()) return fail(LAI_EINVAL, "lai_basis_create: all coefficients zero");
+    sh.func = b->nbf;
+    b->nbf += lai::ncart(sh.l);
+    b->shells.push_back(std::move(sh));
+  }
+  *out = b.release();
+  return LAI_OK;
+}
+
+void lai_basis_destroy(lai_basis* basis) { delete basis; }
+long lai_basis_nbf(const lai_basis* basis) { return basis ? basis->nbf : 0; }
+int lai_basis_nshell(const lai_basis* basis) { return basis ? (int)basis->shells.size() : 0; }
+
+int lai_basis_shell(const lai_basis* basis, int s, int* l, int* nprim, double* center,
+                    double* exps, double* coefs, long* func_index) {
+  if (!basis || s < 0 || s >= (int)basis->shells.size())
+    return fail(LAI_EINVAL, "lai_basis_shell: bad shell index");
+  const HostShell& sh = basis->shells[s];
+  if (l) *l = sh.l;
+  if (nprim) *nprim = (int)sh.exps_all.size();
+  if (center) for (int x = 0; x < 3; ++x) center[x] = sh.center[x];
+  if (exps) std::copy(sh.exps_all.begin(), sh.exps_all.end(), exps);
+  if (coefs) std::copy(sh.coefs_all.begin(), sh.coefs_all.end(), coefs);
+  if (func_index) *func_index = sh.func;
+  return LAI_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+namespace {
+
+struct PairClassHost {
+  int la, lb, Ka, Kb;
+  std::vector<int> sa, sb, fa, fb;  // shell and function indices (oriented)
+  std::vector<double> Q;
+  std::vector<double> AB;          // SoA [3][n]
+  std::vector<double> prim;        // SoA [PF_COUNT][Kab][n]
+  int n() const { return (int)sa.size(); }
+  // device copies
+  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_prim;
+  lai::PairClassDev view() const {
+    lai::PairClassDev v;
+    v.la = la; v.lb = lb; v.Ka = Ka; v.Kb = Kb; v.npairs = n();
+    v.shell_a = d_sa.as<int>(); v.shell_b = d_sb.as<int>();
+    v.func_a = d_fa.as<int>(); v.func_b = d_fb.as<int>();
+    v.Q = d_Q.as<double>(); v.AB = d_AB.as<double>(); v.prim = d_prim.as<double>();
+    return v;
+  }
+};
+
+struct ClassPairBlock {
+  int bra, ket;                 // class indices, bra >= ket
+  std::vector<int64_t> offsets; // host copy
+  DevBuf d_offsets;
+  int64_t total = 0;
+  double alg_flops = 0;         // per quartet of this block
+};
+
+// Algorithmic FP work of one canonical quartet (one unit), the single accounting
+// used for roofline fractions:  P (40 + 64 n + n (20 + T2D + 4 Ncart)) + 25 Ncart
+// with P the product of nonzero primitive counts, n the root count and
+// T2D = 3 [5 (La+Lb+1)(Lc+Ld+1) + 2 Lb (La+Lb+1)(Lc+Ld+1)(Ld+1) + 2 Ld (La+1)(Lb+1)(Lc+Ld+1)].
+double alg_work(int la, int lb, int lc, int ld, int Ka, int Kb, int Kc, int Kd) {
+  const double P = (double)Ka * Kb * Kc * Kd;
+  const int n = (la + lb + lc + ld) / 2 + 1;
+  const double nc = (double)lai::ncart(la) * lai::ncart(lb) * lai::ncart(lc) * lai::ncart(ld);
+  const double t2d = 3.0 * (5.0 * (la + lb + 1) * (lc + ld + 1) +
+                            2.0 * lb * (la + lb + 1) * (lc + ld + 1) * (ld + 1) +
+                            2.0 * ld * (la + 1) * (lb + 1) * (lc + ld + 1));
+  return P * (40.0 + 64.0 * n + n * (20.0 + t2d + 4.0 * nc)) + 25.0 * nc;
+}
+
+__global__ void symmetrize_kernel(const double* __restrict__ Jp, const double* __restrict__ Kp,
+                                  double* __restrict__ J, double* __restrict__ K, int n) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * n) return;
+  const int i = (int)(idx / n), j = (int)(idx - (int64_t)i * n);
+  const int64_t tr = (int64_t)j * n + i;
+  J[idx] = Jp[idx] + Jp[tr];
+  K[idx] = Kp[idx] + Kp[tr];
+}
+
+}  // namespace
+
+struct lai_engine {
+  const lai_basis* basis = nullptr;
+  int device = 0;
+  int num_sms = 148;
+  double thr = 1e-12;
+  cudaStream_t stream = nullptr;
+  DevBuf d_coef, d_hx2, d_hw, d_boys;
+  lai::RysTablesView tab{};
+  std::vector<std::unique_ptr<PairClassHost>> classes;
+  std::vector<std::unique_ptr<ClassPairBlock>> blocks;
+  std::vector<double> Q_all;     // nshell x nshell Schwarz matrix
+  DevBuf d_Jp, d_Kp, d_D, d_J, d_K;
+  DevBuf d_scratch;
+  size_t scratch_doubles = 0;
+  DevBuf d_status;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~lai_engine() {
+    classes.clear();
+    blocks.clear();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int build_classes(lai_engine* E) {
+  const auto& sh = E->basis->shells;
+  const int ns = (int)sh.size();
+  // class key -> index
+  std::vector<std::array<int, 4>> keys;
+  auto class_of = [&](int la, int lb, int Ka, int Kb) {
+    std::array<int, 4> k{la, lb, Ka, Kb};
+    for (size_t i = 0; i < keys.size(); ++i)
+      if (keys[i] == k) return (int)i;
+    keys.push_back(k);
+    E->classes.push_back(std::make_unique<PairClassHost>());
+    auto& c = *E->classes.back();
+    c.la = la; c.lb = lb; c.Ka = Ka; c.Kb = Kb;
+    return (int)keys.size() - 1;
+  };
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j <= i; ++j) {
+      int a = i, b = j;
+      const int Ki = (int)sh[i].exps.size(), Kj = (int)sh[j].exps.size();
+      // orient: higher l first, then more primitives first
+      if (sh[j].l > sh[i].l || (sh[j].l == sh[i].l && Kj > Ki)) std::swap(a, b);
+      const HostShell& A = sh[a];
+      const HostShell& B = sh[b];
+      const int ci = class_of(A.l, B.l, (int)A.exps.size(), (int)B.exps.size());
+      auto& c = *E->classes[ci];
+      c.sa.push_back(a); c.sb.push_back(b);
+      c.fa.push_back((int)A.func); c.fb.push_back((int)B.func);
+    }
+  // sort classes by key so that bra >= ket implies (la,lb) >= (lc,ld)
+  std::vector<int> order(keys.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::sort(order.begin(), order.end(), [&](int x, int y) { return keys[x] < keys[y]; });
+  std::vector<std::unique_ptr<PairClassHost>> sorted;
+  for (int o : order) sorted.push_back(std::move(E->classes[o]));
+  E->classes = std::move(sorted);
+  return LAI_OK;
+}
+
+void fill_pair_data(const lai_basis* basis, PairClassHost& c) {
+  const auto& sh = basis->shells;
+  const int n = c.n();
+  const int Kab = c.Ka * c.Kb;
+  c.AB.assign(3 * (size_t)n, 0.0);
+  c.prim.assign((size_t)lai::PF_COUNT * Kab * n, 0.0);
+  const double pi54s2 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
+  for (int p = 0; p < n; ++p) {
+    const HostShell& A = sh[c.sa[p]];
+    const HostShell& B = sh[c.sb[p]];
+    double AB[3], ab2 = 0;
+    for (int x = 0; x < 3; ++x) {
+      AB[x] = A.center[x] - B.center[x];
+      ab2 += AB[x] * AB[x];
+      c.AB[(size_t)x * n + p] = AB[x];
+    }
+    for (int ia = 0; ia < c.Ka; ++ia)
+      for (int ib = 0; ib < c.Kb; ++ib) {
+        const int t = ia * c.Kb + ib;
+        const double al = A.exps[ia], be = B.exps[ib];
+        const double z = al + be;
+        auto at = [&](int f) -> double& { return c.prim[((size_t)f * Kab + t) * n + p]; };
+        at(lai::PF_ZETA) = z;
+        at(lai::PF_HZ) = 0.5 / z;
+        for (int x = 0; x < 3; ++x) {
+          const double P = (al * A.center[x] + be * B.center[x]) / z;
+          at(lai::PF_PX + x) = P;
+          at(lai::PF_PAX + x) = P - A.center[x];
+        }
+        at(lai::PF_C) = pi54s2 * A.coefs[ia] * B.coefs[ib] * std::exp(-al * be / z * ab2) / z;
+      }
+  }
+}
+
+int upload_class(PairClassHost& c) {
+  LAI_CUDA_TRY(upload(c.d_sa, c.sa));
+  LAI_CUDA_TRY(upload(c.d_sb, c.sb));
+  LAI_CUDA_TRY(upload(c.d_fa, c.fa));
+  LAI_CUDA_TRY(upload(c.d_fb, c.fb));
+  LAI_CUDA_TRY(upload(c.d_AB, c.AB));
+  LAI_CUDA_TRY(upload(c.d_prim, c.prim));
+  if (c.Q.empty()) c.Q.assign(c.n(), 0.0);
+  LAI_CUDA_TRY(upload(c.d_Q, c.Q));
+  return LAI_OK;
+}
+
+int ensure_scratch(lai_engine* E, size_t doubles) {
+  if (doubles <= E->scratch_doubles) return LAI_OK;
+  LAI_CUDA_TRY(E->d_scratch.alloc(doubles * sizeof(double)));
+  E->scratch_doubles = doubles;
+  return LAI_OK;
+}
+
+int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs& args) {
+  const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
+  if (lai::small_class_supported(la, lb, lc, ld)) {
+    const int rc = lai::launch_small(blk, args, E->tab, E->stream, false);
+    if (rc < 0) return fail(LAI_ECUDA, std::string("small-class launch failed: ") +
+                                           cudaGetErrorString(cudaGetLastError()));
+    return LAI_OK;
+  }
+  const size_t need = lai::generic_global_scratch_doubles(la, lb, lc, ld, E->num_sms);
+  if (int rc = ensure_scratch(E, need)) return rc;
+  const int rc = lai::launch_generic(blk, args, E->tab, E->stream, E->d_scratch.as<double>(),
+                                     E->scratch_doubles, E->num_sms);
+  if (rc < 0) return fail(LAI_ECUDA, std::string("generic launch failed: ") +
+                                         cudaGetErrorString(cudaGetLastError()));
+  return LAI_OK;
+}
+
+int compute_schwarz(lai_engine* E) {
+  // Diagonal quartets (ab|ab) of every pair: offsets[p] = p, qbegin[p] = p.
+  for (auto& cp : E->classes) {
+    auto& c = *cp;
+    const int n = c.n();
+    std::vector<int64_t> off(n + 1);
+    std::vector<int> qb(n);
+    for (int p = 0; p <= n; ++p) off[p] = p;
+    for (int p = 0; p < n; ++p) qb[p] = p;
+    DevBuf d_off, d_qb, d_out;
+    LAI_CUDA_TRY(upload(d_off, off));
+    LAI_CUDA_TRY(upload(d_qb, qb));
+    LAI_CUDA_TRY(d_out.alloc(sizeof(double) * n));
+    lai::QuartetBlock blk{};
+    blk.bra = blk.ket = c.view();
+    blk.offsets = d_off.as<int64_t>();
+    blk.qbegin = d_qb.as<int>();
+    blk.total = n;
+    blk.same_class = 1;
+    lai::JKArgs args{};
+    args.mode = lai::MODE_SCHWARZ;
+    args.schwarz_out = d_out.as<double>();
+    if (int rc = launch_block(E, blk, args)) return rc;
+    c.Q.resize(n);
+    LAI_CUDA_TRY(cudaMemcpyAsync(c.Q.data(), d_out.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                 E->stream));
+    LAI_CUDA_TRY(cudaStreamSynchronize(E->stream));
+  }
+  return LAI_OK;
+}
+
+int sort_and_screen(lai_engine* E) {
+  const int ns = (int)E->basis->shells.size();
+  E->Q_all.assign((size_t)ns * ns, 0.0);
+  double qmax = 0.0;
+  for (auto& cp : E->classes)
+    for (int p = 0; p < cp->n(); ++p) {
+      qmax = std::max(qmax, cp->Q[p]);
+      E->Q_all[(size_t)cp->sa[p] * ns + cp->sb[p]] = cp->Q[p];
+      E->Q_all[(size_t)cp->sb[p] * ns + cp->sa[p]] = cp->Q[p];
+    }
+  for (auto& cp : E->classes) {
+    auto& c = *cp;
+    const int n = c.n();
+    std::vector<int> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return c.Q[x] > c.Q[y]; });
+    int keep = 0;
+    while (keep < n && c.Q[idx[keep]] * qmax >= E->thr) ++keep;
+    const int Kab = c.Ka * c.Kb;
+    auto perm = [&](const std::vector<int>& v) {
+      std::vector<int> o(keep);
+      for (int i = 0; i < keep; ++i) o[i] = v[idx[i]];
+      return o;
+    };
+    std::vector<double> Q(keep), AB(3 * (size_t)keep), prim((size_t)lai::PF_COUNT * Kab * keep);
+    for (int i = 0; i < keep; ++i) {
+      Q[i] = c.Q[idx[i]];
+      for (int x = 0; x < 3; ++x) AB[(size_t)x * keep + i] = c.AB[(size_t)x * n + idx[i]];
+      for (int f = 0; f < lai::PF_COUNT * Kab; ++f)
+        prim[(size_t)f * keep + i] = c.prim[(size_t)f * n + idx[i]];
+    }
+    c.sa = perm(c.sa); c.sb = perm(c.sb); c.fa = perm(c.fa); c.fb = perm(c.fb);
+    c.Q = std::move(Q); c.AB = std::move(AB); c.prim = std::move(prim);
+    if (int rc = upload_class(c)) return rc;
+  }
+  // quartet blocks
+  const int nc = (int)E->classes.size();
+  for (int A = 0; A < nc; ++A)
+    for (int B = 0; B <= A; ++B) {
+      const auto& ca = *E->classes[A];
+      const auto& cb = *E->classes[B];
+      if (ca.n() == 0 || cb.n() == 0) continue;
+      auto blk = std::make_unique<ClassPairBlock>();
+      blk->bra = A;
+      blk->ket = B;
+      blk->offsets.resize(ca.n() + 1);
+      blk->offsets[0] = 0;
+      for (int p = 0; p < ca.n(); ++p) {
+        // largest prefix of the ket list with Q_p * Q_q >= thr
+        int lo = 0, hi = cb.n();
+        while (lo < hi) {
+          const int mid = (lo + hi) / 2;
+          if (ca.Q[p] * cb.Q[mid] >= E->thr) lo = mid + 1; else hi = mid;
+        }
+        int cnt = lo;
+        if (A == B) cnt = std::min(cnt, p + 1);
+        blk->offsets[p + 1] = blk->offsets[p] + cnt;
+      }
+      blk->total = blk->offsets[ca.n()];
+      if (blk->total == 0) continue;
+      blk->alg_flops = alg_work(ca.la, ca.lb, cb.la, cb.lb, ca.Ka, ca.Kb, cb.Ka, cb.Kb);
+      LAI_CUDA_TRY(upload(blk->d_offsets, blk->offsets));
+      E->blocks.push_back(std::move(blk));
+    }
+  return LAI_OK;
+}
+
+lai::QuartetBlock make_block(const lai_engine* E, const ClassPairBlock& b) {
+  lai::QuartetBlock q{};
+  q.bra = E->classes[b.bra]->view();
+  q.ket = E->classes[b.ket]->view();
+  q.offsets = b.d_offsets.as<int64_t>();
+  q.qbegin = nullptr;
+  q.total = b.total;
+  q.same_class = (b.bra == b.ket);
+  return q;
+}
+
+int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t stream,
+           lai_jk_report* rep, bool timed) {
+  const int nbf = (int)E->basis->nbf;
+  const size_t bytes = sizeof(double) * (size_t)nbf * nbf;
+  if (E->d_Jp.bytes < bytes) {
+    LAI_CUDA_TRY(E->d_Jp.alloc(bytes));
+    LAI_CUDA_TRY(E->d_Kp.alloc(bytes));
+  }
+  cudaStream_t saved = E->stream;
+  E->stream = stream;
+  LAI_CUDA_TRY(cudaMemsetAsync(E->d_Jp.p, 0, bytes, stream));
+  LAI_CUDA_TRY(cudaMemsetAsync(E->d_Kp.p, 0, bytes, stream));
+  if (timed) LAI_CUDA_TRY(cudaEventRecord(E->ev0, stream));
+  lai::JKArgs args{};
+  args.D = dD;
+  args.J = E->d_Jp.as<double>();
+  args.K = E->d_Kp.as<double>();
+  args.nbf = nbf;
+  args.mode = lai::MODE_JK;
+  int launches = 0;
+  int64_t nq = 0;
+  double flops = 0;
+  for (auto& bp : E->blocks) {
+    const lai::QuartetBlock q = make_block(E, *bp);
+    if (int rc = launch_block(E, q, args)) { E->stream = saved; return rc; }
+    ++launches;
+    nq += bp->total;
+    flops += bp->alg_flops * (double)bp->total;
+  }
+  const int64_t nn = (int64_t)nbf * nbf;
+  if (nn > 0) {
+    symmetrize_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(
+        E->d_Jp.as<double>(), E->d_Kp.as<double>(), dJ, dK, nbf);
+    ++launches;
+  }
+  LAI_CUDA_TRY(cudaGetLastError());
+  if (timed) LAI_CUDA_TRY(cudaEventRecord(E->ev1, stream));
+  E->stream = saved;
+  if (rep) {
+    rep->quartets_fp64 = nq;
+    rep->quartets_fp32 = 0;
+    rep->alg_flops = flops;
+    rep->kernel_launches = launches;
+    rep->seconds_device = 0;
+  }
+  return LAI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void lai_engine_opts_default(lai_engine_opts* opts) {
+  if (!opts) return;
+  opts->schwarz_threshold = 1e-12;
+  opts->device = 0;
+}
+
+void lai_jk_opts_default(lai_jk_opts* opts) {
+  if (!opts) return;
+  opts->fp32_cut = 0.0;
+  opts->check_symmetric = 0;
+}
+
+int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_engine** out) {
+  if (!out || !basis) return fail(LAI_EINVAL, "lai_engine_create: null argument");
+  *out = nullptr;
+  lai_engine_opts o;
+  lai_engine_opts_default(&o);
+  if (opts) o = *opts;
+  if (!(o.schwarz_threshold >= 0.0)) return fail(LAI_EINVAL, "negative Schwarz threshold");
+  int ndev = 0;
+  LAI_CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (o.device < 0 || o.device >= ndev) return fail(LAI_EINVAL, "lai_engine_create: bad device");
+  LAI_CUDA_TRY(cudaSetDevice(o.device));
+  auto E = std::make_unique<lai_engine>();
+  E->basis = basis;
+  E->device = o.device;
+  E->thr = o.schwarz_threshold;
+  LAI_CUDA_TRY(cudaDeviceGetAttribute(&E->num_sms, cudaDevAttrMultiProcessorCount, o.device));
+  LAI_CUDA_TRY(cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking));
+  LAI_CUDA_TRY(cudaEventCreate(&E->ev0));
+  LAI_CUDA_TRY(cudaEventCreate(&E->ev1));
+  {
+    std::vector<double> coef(RYS_COEF_H, RYS_COEF_H + RYS_COEF_LEN);
+    std::vector<double> hx(RYS_HERM_X2_H, RYS_HERM_X2_H + RYS_HERM_LEN);
+    std::vector<double> hw(RYS_HERM_W_H, RYS_HERM_W_H + RYS_HERM_LEN);
+    std::vector<double> bg(BOYS_GRID_H, BOYS_GRID_H + BOYS_NGRID * BOYS_NM);
+    LAI_CUDA_TRY(upload(E->d_coef, coef));
+    LAI_CUDA_TRY(upload(E->d_hx2, hx));
+    LAI_CUDA_TRY(upload(E->d_hw, hw));
+    LAI_CUDA_TRY(upload(E->d_boys, bg));
+    E->tab = {E->d_coef.as<double>(), E->d_hx2.as<double>(), E->d_hw.as<double>(),
+              E->d_boys.as<double>()};
+  }
+  if (int rc = build_classes(E.get())) return rc;
+  for (auto& c : E->classes) {
+    fill_pair_data(basis, *c);
+    if (int rc = upload_class(*c)) return rc;
+  }
+  if (int rc = compute_schwarz(E.get())) return rc;
+  if (int rc = sort_and_screen(E.get())) return rc;
+  *out = E.release();
+  return LAI_OK;
+}
+
+void lai_engine_destroy(lai_engine* engine) {
+  if (engine) {
+    cudaSetDevice(engine->device);
+    delete engine;
+  }
+}
+
+int lai_engine_schwarz(lai_engine* engine, double* Q) {
+  if (!engine || !Q) return fail(LAI_EINVAL, "lai_engine_schwarz: null argument");
+  std::copy(engine->Q_all.begin(), engine->Q_all.end(), Q);
+  return LAI_OK;
+}
+
+int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d_J, double* d_K,
+                        void* stream, const lai_jk_opts* opts, lai_jk_report* report) {
+  if (!engine || !d_D || !d_J || !d_K) return fail(LAI_EINVAL, "lai_jk_build_device: null argument");
+  lai_jk_opts o;
+  lai_jk_opts_default(&o);
+  if (opts) o = *opts;
+  if (o.fp32_cut != 0.0) return fail(LAI_ENOTSUP, "mixed precision not enabled in this build");
+  LAI_CUDA_TRY(cudaSetDevice(engine->device));
+  return run_jk(engine, d_D, d_J, d_K, (cudaStream_t)stream, report, false);
+}
+
+int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double* J, double* K,
+                 const lai_jk_opts* opts, lai_jk_report* report) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (!engine || !D || !J || !K) return fail(LAI_EINVAL, "lai_jk_build: null argument");
+  if ((long)nbf != engine->basis->nbf)
+    return fail(LAI_EINVAL, "lai_jk_build: nbf mismatch (expected " +
+                                std::to_string(engine->basis->nbf) + ", got " +
+                                std::to_string(nbf) + ")");
+  lai_jk_opts o;
+  lai_jk_opts_default(&o);
+  if (opts) o = *opts;
+  if (o.fp32_cut != 0.0) return fail(LAI_ENOTSUP, "mixed precision not enabled in this build");
+  if (o.check_symmetric) {
+    for (size_t i = 0; i < nbf; ++i)
+      for (size_t j = 0; j < i; ++j)
+        if (std::fabs(D[i * nbf + j] - D[j * nbf + i]) > 1e-12 * (1.0 + std::fabs(D[i * nbf + j])))
+          return fail(LAI_EINVAL, "lai_jk_build: density matrix is not symmetric");
+  }
+  LAI_CUDA_TRY(cudaSetDevice(engine->device));
+  const size_t bytes = sizeof(double) * nbf * nbf;
+  if (engine->d_D.bytes < bytes) {
+    LAI_CUDA_TRY(engine->d_D.alloc(bytes));
+    LAI_CUDA_TRY(engine->d_J.alloc(bytes));
+    LAI_CUDA_TRY(engine->d_K.alloc(bytes));
+  }
+  cudaStream_t s = engine->stream;
+  LAI_CUDA_TRY(cudaMemcpyAsync(engine->d_D.p, D, bytes, cudaMemcpyHostToDevice, s));
+  if (int rc = run_jk(engine, engine->d_D.as<double>(), engine->d_J.as<double>(),
+                      engine->d_K.as<double>(), s, report, true))
+    return rc;
+  LAI_CUDA_TRY(cudaMemcpyAsync(J, engine->d_J.p, bytes, cudaMemcpyDeviceToHost, s));
+  LAI_CUDA_TRY(cudaMemcpyAsync(K, engine->d_K.p, bytes, cudaMemcpyDeviceToHost, s));
+  LAI_CUDA_TRY(cudaStreamSynchronize(s));
+  if (report) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, engine->ev0, engine->ev1);
+    report->seconds_device = ms * 1e-3;
+    report->seconds_total =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return LAI_OK;
+}
+
+int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_capacity,
+                           lai_quartet_meta* meta, size_t meta_capacity, int64_t* n_quartets,
+                           int64_t* n_values) {
+  if (!engine) return fail(LAI_EINVAL, "lai_eri_batch_screened: null engine");
+  int64_t nq = 0, nv = 0;
+  std::vector<int64_t> vals_per(engine->blocks.size());
+  for (size_t b = 0; b < engine->blocks.size(); ++b) {
+    const auto& bp = *engine->blocks[b];
+    const auto& ca = *engine->classes[bp.bra];
+    const auto& cb = *engine->classes[bp.ket];
+    vals_per[b] = (int64_t)lai::ncart(ca.la) * lai::ncart(ca.lb) * lai::ncart(cb.la) * lai::ncart(cb.lb);
+    nq += bp.total;
+    nv += bp.total * vals_per[b];
+  }
+  if (n_quartets) *n_quartets = nq;
+  if (n_values) *n_values = nv;
+  if (!out || !meta) return LAI_OK;
+  if ((int64_t)out_capacity < nv || (int64_t)meta_capacity < nq)
+    return fail(LAI_EINVAL, "lai_eri_batch_screened: output capacity too small");
+  LAI_CUDA_TRY(cudaSetDevice(engine->device));
+  DevBuf d_out, d_meta;
+  LAI_CUDA_TRY(d_out.alloc(sizeof(double) * (size_t)std::max<int64_t>(nv, 1)));
+  LAI_CUDA_TRY(d_meta.alloc(sizeof(int) * 4 * (size_t)std::max<int64_t>(nq, 1)));
+  int64_t qo = 0, vo = 0;
+  for (size_t b = 0; b < engine->blocks.size(); ++b) {
+    const auto& bp = *engine->blocks[b];
+    lai::JKArgs args{};
+    args.mode = lai::MODE_RAW;
+    args.raw_out = d_out.as<double>() + vo;
+    args.raw_meta = d_meta.as<int>() + 4 * qo;
+    if (int rc = launch_block(engine, make_block(engine, bp), args)) return rc;
+    qo += bp.total;
+    vo += bp.total * vals_per[b];
+  }
+  std::vector<int> hmeta(4 * (size_t)nq);
+  LAI_CUDA_TRY(cudaMemcpyAsync(out, d_out.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, engine->stream));
+  LAI_CUDA_TRY(cudaMemcpyAsync(hmeta.data(), d_meta.p, sizeof(int) * 4 * nq, cudaMemcpyDeviceToHost,
+                               engine->stream));
+  LAI_CUDA_TRY(cudaStreamSynchronize(engine->stream));
+  qo = 0;
+  vo = 0;
+  for (size_t b = 0; b < engine->blocks.size(); ++b) {
+    const auto& bp = *engine->blocks[b];
+    const auto& ca = *engine->classes[bp.bra];
+    const auto& cb = *engine->classes[bp.ket];
+    for (int64_t t = 0; t < bp.total; ++t) {
+      lai_quartet_meta& m = meta[qo + t];
+      m.offset = vo + t * vals_per[b];
+      m.fa = hmeta[4 * (qo + t)]; m.fb = hmeta[4 * (qo + t) + 1];
+      m.fc = hmeta[4 * (qo + t) + 2]; m.fd = hmeta[4 * (qo + t) + 3];
+      m.na = lai::ncart(ca.la); m.nb = lai::ncart(ca.lb);
+      m.nc = lai::ncart(cb.la); m.nd = lai::ncart(cb.lb);
+    }
+    qo += bp.total;
+    vo += bp.total * vals_per[b];
+  }
+  return LAI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,120 @@
+// Device-side building blocks shared by the ERI/J-K kernels.
+//
+// Algorithm (per contracted shell quartet (ab|cd), la>=lb, lc>=ld):
+//   1. For each primitive quartet and each Rys root u_r (weight w_r), build the
+//      2D tables I_x(e, f), I_y, I_z for e <= la+lb, f <= lc+ld by the vertical
+//      recurrence of the reference's build_2d_rys (src/host/kernels/eri_kernel.cpp:
+//      119-141):
+//        I(e+1,0) = PA' I(e,0) + e B10 I(e-1,0)
+//        I(e,f+1) = QC' I(e,f) + f B01 I(e,f-1) + e B00 I(e-1,f)
+//      with PA' = PA - (eta/(zeta+eta)) u PQ, QC' = QC + (zeta/(zeta+eta)) u PQ,
+//      B10 = (1 - eta u/(zeta+eta))/(2 zeta), B01 = (1 - zeta u/(zeta+eta))/(2 eta),
+//      B00 = u/(2(zeta+eta)) (eri_kernel.cpp:302-317).
+//   2. Accumulate G[e][f] = sum_{prim,r} w_r pref I_x I_y I_z over the Cartesian
+//      components e of shells la..la+lb and f of lc..lc+ld -- the "(e0|f0)"
+//      integrals, contracted over primitives BEFORE the horizontal transfer.
+//   3. Horizontal transfer once per contracted quartet, in closed (binomial) form:
+//      (a b| = sum_{k<=b} prod_x C(b_x,k_x) (A-B)_x^{b_x-k_x} (a+k 0|, same for |c d),
+//      which equals the reference's HRR I(a,b+1) = I(a+1,b) + AB I(a,b)
+//      (eri_kernel.cpp:143-163) applied in each direction.
+//   4. Per-component normalization 1/sqrt((2lx-1)!!(2ly-1)!!(2lz-1)!!)
+//      (include/libaccint/kernels/norm_correction.hpp:28-34).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lai_common.h"
+#include "rys_eval.h"
+
+namespace lai {
+
+constexpr int kMaxCartL = 9;                  // components tabulated up to l = 9
+constexpr int kNCartMax = 55;                 // (9+1)(9+2)/2
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+// Number of components of shells lo..hi.
+__host__ __device__ constexpr int ncart_range(int lo, int hi) {
+  return ((hi + 1) * (hi + 2) * (hi + 3) - lo * (lo + 1) * (lo + 2)) / 6;
+}
+// Index of (lx, ly, lz) inside its shell: lx descending, then ly descending.
+__host__ __device__ constexpr int cart_index(int lx, int ly, int lz) {
+  return ((ly + lz) * (ly + lz + 1)) / 2 + lz;
+}
+// Offset of shell l inside a component list that starts at shell lo.
+__host__ __device__ constexpr int ncart_before(int lo, int l) { return ncart_range(lo, l) - ncart(l); }
+
+// Packed component (lx | ly << 4 | lz << 8) of the i-th Cartesian function of shell l.
+__host__ __device__ constexpr int cart_comp(int l, int i) {
+  int k = 0;
+  for (int x = l; x >= 0; --x)
+    for (int y = l - x; y >= 0; --y) {
+      if (k == i) return x | (y << 4) | ((l - x - y) << 8);
+      ++k;
+    }
+  return 0;
+}
+__host__ __device__ constexpr int comp_x(int c) { return c & 15; }
+__host__ __device__ constexpr int comp_y(int c) { return (c >> 4) & 15; }
+__host__ __device__ constexpr int comp_z(int c) { return (c >> 8) & 15; }
+
+__host__ __device__ constexpr double dfact_odd(int l) {  // (2l-1)!!
+  double r = 1;
+  for (int k = 2 * l - 1; k > 1; k -= 2) r *= k;
+  return r;
+}
+__host__ __device__ constexpr double binom(int n, int k) {
+  double r = 1;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+
+// Per-component normalization factor of component i of shell l.
+__device__ __forceinline__ double norm_factor(int l, int i) {
+  const int c = cart_comp(l, i);
+  return rsqrt(dfact_odd(comp_x(c)) * dfact_odd(comp_y(c)) * dfact_odd(comp_z(c)));
+}
+
+// x^m for small non-negative m.
+template <typename R>
+__device__ __forceinline__ R ipow(R x, int m) {
+  R r = R(1);
+  for (int i = 0; i < m; ++i) r *= x;
+  return r;
+}
+
+// Arguments of one J/K (or raw-integral) launch.
+struct JKArgs {
+  const double* D;       // nbf x nbf density, row-major (symmetric)
+  double* J;             // nbf x nbf, receives the un-symmetrized J' (J = J' + J'^T)
+  double* K;             // nbf x nbf, receives the un-symmetrized K' (K = K' + K'^T)
+  int nbf;
+  int mode;              // MODE_JK, MODE_RAW, MODE_SCHWARZ
+  double* raw_out;       // MODE_RAW: [quartet][a][b][c][d]
+  int* raw_meta;         // MODE_RAW: [quartet][4] first function index of a, b, c, d
+  double* schwarz_out;   // MODE_SCHWARZ: [bra pair] sqrt(max |(ab|ab)|)
+  unsigned int* status;  // device status word (0 = ok)
+};
+enum { MODE_JK = 0, MODE_RAW = 1, MODE_SCHWARZ = 2 };
+
+// Locate the bra pair p of flat quartet index t: largest p with offsets[p] <= t.
+__device__ __forceinline__ int find_bra(const int64_t* __restrict__ offsets, int npairs, int64_t t) {
+  int lo = 0, hi = npairs;  // offsets[lo] <= t < offsets[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(offsets + mid) <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Degeneracy weight of a canonical quartet for the 8-fold symmetric scatter:
+// 1/2 for each of i==j, k==l, (ij)==(kl) (the permutation flags of the reference's
+// accumulate_symmetric, src/shared/consumers/fock_builder.cpp:123-222).
+__device__ __forceinline__ double quartet_weight(const QuartetBlock& blk, int p, int q) {
+  double s = 1.0;
+  if (__ldg(blk.bra.shell_a + p) == __ldg(blk.bra.shell_b + p)) s *= 0.5;
+  if (__ldg(blk.ket.shell_a + q) == __ldg(blk.ket.shell_b + q)) s *= 0.5;
+  if (blk.same_class && p == q) s *= 0.5;
+  return s;
+}
+
+}  // namespace lai

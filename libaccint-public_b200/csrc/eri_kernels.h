@@ -1,0 +1,24 @@
+// Launch entry points of the ERI/J-K kernels (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "eri_device.cuh"
+
+namespace lai {
+
+// Thread-per-quartet kernels for the small classes (eri_small.cu).  Returns 1 if
+// the class (la,lb|lc,ld) has a specialised kernel and it was launched, 0 if the
+// class is not covered (use the generic kernel), <0 on a launch error.
+int launch_small(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
+                 cudaStream_t stream, bool fp32);
+bool small_class_supported(int la, int lb, int lc, int ld);
+
+// Warp-per-quartet generic kernel (eri_generic.cu), any class with l <= 4.
+int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
+                   cudaStream_t stream, double* gscratch, size_t gscratch_doubles, int num_sms);
+// Global scratch (doubles) the generic kernel needs for class (la,lb|lc,ld) when
+// its (e0|f0) block does not fit in shared memory; 0 if it fits.
+size_t generic_global_scratch_doubles(int la, int lb, int lc, int ld, int num_sms);
+
+}  // namespace lai

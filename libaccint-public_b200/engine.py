@@ -1,0 +1,190 @@
+"""Python surface mirroring the reference's operator/consumer API for the J/K path.
+
+    basis = BasisSet.from_atoms(Z, xyz, "cc-pvdz")
+    engine = Engine(basis)
+    fb = FockBuilder(basis.nbf)
+    fb.set_density(D)
+    engine.compute(Operator.coulomb(), fb)          # Engine::compute(op, FockBuilder&)
+    J, K = fb.get_coulomb_matrix(), fb.get_exchange_matrix()
+
+Reference counterparts: Engine (include/libaccint/engine/engine.hpp:86-107,
+435-499, 727-731, 1635-1666), FockBuilder (include/libaccint/consumers/fock_builder.hpp,
+src/shared/consumers/fock_builder.cpp), ScreeningOptions
+(include/libaccint/screening/screening_options.hpp).  Every call goes through the
+C ABI of libaccint_b200.so; there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+class Operator:
+    """Only the Coulomb two-electron operator is on this path."""
+
+    def __init__(self, kind):
+        self.kind = kind
+
+    @staticmethod
+    def coulomb():
+        return Operator("coulomb")
+
+    def is_two_electron(self):
+        return self.kind == "coulomb"
+
+
+class ScreeningOptions:
+    def __init__(self, threshold=1e-12, enabled=True, use_permutation_symmetry=True):
+        self.threshold = threshold
+        self.enabled = enabled
+        self.use_permutation_symmetry = use_permutation_symmetry
+
+    @staticmethod
+    def normal():
+        return ScreeningOptions(1e-12)
+
+    @staticmethod
+    def tight():
+        return ScreeningOptions(1e-14)
+
+    @staticmethod
+    def loose():
+        return ScreeningOptions(1e-10)
+
+
+class FockBuilder:
+    """J/K accumulator (reference consumers::FockBuilder).  J and K accumulate
+    across compute calls until reset(), like the reference's J_/K_ buffers."""
+
+    def __init__(self, nbf):
+        self.nbf = int(nbf)
+        self.J = np.zeros((self.nbf, self.nbf))
+        self.K = np.zeros((self.nbf, self.nbf))
+        self.D = None
+        self.last_report = None
+
+    def set_density(self, D, nbf=None):
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        n = D.shape[0] if nbf is None else int(nbf)
+        if n != self.nbf or D.shape != (self.nbf, self.nbf):
+            raise ValueError(f"FockBuilder::set_density: nbf mismatch (expected {self.nbf}, got {n})")
+        self.D = D
+
+    def get_coulomb_matrix(self):
+        return self.J
+
+    def get_exchange_matrix(self):
+        return self.K
+
+    def get_fock_matrix(self, H_core, exchange_fraction=0.5):
+        H = np.asarray(H_core, dtype=np.float64).reshape(self.nbf, self.nbf)
+        return H + self.J - exchange_fraction * self.K
+
+    def reset(self):
+        self.J[:] = 0.0
+        self.K[:] = 0.0
+
+
+class Engine:
+    def __init__(self, basis, threshold=1e-12, device=0):
+        self.basis = basis
+        self.threshold = threshold
+        L = _lib.lib()
+        opts = _lib.EngineOpts()
+        L.lai_engine_opts_default(ctypes.byref(opts))
+        opts.schwarz_threshold = threshold
+        opts.device = device
+        h = ctypes.c_void_p()
+        _lib.check(L.lai_engine_create(basis.handle(), ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+
+    def schwarz(self):
+        n = self.basis.n_shells
+        Q = np.zeros((n, n))
+        _lib.check(_lib.lib().lai_engine_schwarz(self._h, Q.ctypes.data))
+        return Q
+
+    def jk(self, D, fp32_cut=0.0, check_symmetric=False):
+        """(J, K, report) for a host density D."""
+        L = _lib.lib()
+        n = self.basis.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        if D.shape != (n, n):
+            raise ValueError(f"density must be {n}x{n}")
+        J = np.empty((n, n))
+        K = np.empty((n, n))
+        opts = _lib.JKOpts()
+        L.lai_jk_opts_default(ctypes.byref(opts))
+        opts.fp32_cut = fp32_cut
+        opts.check_symmetric = int(check_symmetric)
+        rep = _lib.JKReport()
+        _lib.check(L.lai_jk_build(self._h, D.ctypes.data, n, J.ctypes.data, K.ctypes.data,
+                                  ctypes.byref(opts), ctypes.byref(rep)))
+        return J, K, rep
+
+    def jk_device(self, d_D, d_J, d_K, stream=0, fp32_cut=0.0):
+        """Device-pointer variant (integers from torch.Tensor.data_ptr())."""
+        L = _lib.lib()
+        opts = _lib.JKOpts()
+        L.lai_jk_opts_default(ctypes.byref(opts))
+        opts.fp32_cut = fp32_cut
+        rep = _lib.JKReport()
+        _lib.check(L.lai_jk_build_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
+                                         ctypes.c_void_p(d_K), ctypes.c_void_p(stream),
+                                         ctypes.byref(opts), ctypes.byref(rep)))
+        return rep
+
+    def compute_batch_screened(self, op=None):
+        """All canonical screened quartets: (values, meta) with meta rows
+        (offset, fa, fb, fc, fd, na, nb, nc, nd) -- the IntegralBuffer layout."""
+        L = _lib.lib()
+        nq = ctypes.c_int64()
+        nv = ctypes.c_int64()
+        _lib.check(L.lai_eri_batch_screened(self._h, None, 0, None, 0, ctypes.byref(nq), ctypes.byref(nv)))
+        out = np.zeros(max(nv.value, 1))
+        meta = (_lib.QuartetMeta * max(nq.value, 1))()
+        _lib.check(L.lai_eri_batch_screened(self._h, out.ctypes.data, out.size, meta, nq.value,
+                                            ctypes.byref(nq), ctypes.byref(nv)))
+        m = np.array([(x.offset, x.fa, x.fb, x.fc, x.fd, x.na, x.nb, x.nc, x.nd)
+                      for x in meta[:nq.value]], dtype=np.int64).reshape(-1, 9)
+        return out[:nv.value], m
+
+    def compute_and_consume(self, op, consumer, screening=None):
+        if not op.is_two_electron():
+            raise ValueError("compute_and_consume requires a two-electron operator")
+        if consumer.D is None:
+            raise RuntimeError("FockBuilder::accumulate called without density matrix")
+        if consumer.nbf != self.basis.nbf:
+            raise ValueError("FockBuilder nbf does not match the basis")
+        if screening is not None and screening.enabled and screening.threshold != self.threshold:
+            raise ValueError("screening threshold differs from the engine's; build an Engine "
+                             "with threshold=%g" % screening.threshold)
+        J, K, rep = self.jk(consumer.D)
+        consumer.J += J
+        consumer.K += K
+        consumer.last_report = rep
+
+    def compute(self, op, consumer):
+        self.compute_and_consume(op, consumer)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.lib().lai_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def jk(basis, D, threshold=1e-12, fp32_cut=0.0):
+    """One-shot J/K for a basis and density."""
+    e = Engine(basis, threshold)
+    try:
+        J, K, _ = e.jk(D, fp32_cut=fp32_cut)
+    finally:
+        e.close()
+    return J, K

@@ -1,0 +1,240 @@
+"""Test infrastructure only: Python access to the two CPU checkers.
+
+* ``restatement()`` -- liboracle.so, the plain-C restatement of the reference
+  algorithm in rys_oracle.c (binary128 Rys roots, double ERIs, serial 8-fold
+  symmetric J/K).  Built by ``make -C oracle restatement`` (no reference tree needed).
+* ``reference()``   -- _ref/libref_oracle.so, the UNMODIFIED reference CPU code
+  compiled from its own sources by oracle/Makefile, behind ref_shim.cpp.  None when
+  it was not built (the reference tree is absent).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
+use this module.  The product (libaccint-public_b200) never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATEMENT = os.path.join(HERE, "liboracle.so")
+REFERENCE = os.path.join(HERE, "_ref", "libref_oracle.so")
+
+_P, _I, _D, _L = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
+_orc = None
+_ref = None
+
+
+def build_restatement():
+    subprocess.run(["make", "-s", "-C", HERE, "restatement"], check=True)
+
+
+def restatement():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(RESTATEMENT) or (
+                os.path.exists(os.path.join(HERE, "rys_oracle.c")) and
+                os.path.getmtime(os.path.join(HERE, "rys_oracle.c")) > os.path.getmtime(RESTATEMENT)):
+            build_restatement()
+        L = ctypes.CDLL(RESTATEMENT)
+        L.orc_boys.argtypes = [_I, _D, _P]
+        L.orc_rys.argtypes = [_I, _D, _P, _P]
+        L.orc_normalize.argtypes = [_I, _I, _P, _P, _P]
+        L.orc_eri_quartet.argtypes = [_P, _P, _P, _P, _P, _P]
+        L.orc_basis_quartet.argtypes = [_I, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P]
+        L.orc_schwarz.argtypes = [_I, _P, _P, _P, _P, _P, _P]
+        L.orc_jk_sym.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _D]
+        L.orc_jk_sym.restype = ctypes.c_long
+        _orc = L
+    return _orc
+
+
+def reference():
+    """The compiled reference, or None if oracle/_ref was not built."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REFERENCE):
+            return None
+        L = ctypes.CDLL(REFERENCE)
+        L.ref_last_error.restype = ctypes.c_char_p
+        L.ref_basis_create.restype = _P
+        L.ref_basis_create.argtypes = [_I, _P, _P, _P, _P, _P, _P]
+        L.ref_basis_builtin_sto3g.restype = _P
+        L.ref_basis_builtin_sto3g.argtypes = [_I, _P, _P]
+        L.ref_basis_free.argtypes = [_P]
+        L.ref_basis_nbf.restype = _L
+        L.ref_basis_nbf.argtypes = [_P]
+        L.ref_basis_nshell.restype = _L
+        L.ref_basis_nshell.argtypes = [_P]
+        L.ref_basis_shell.argtypes = [_P, _L, _P, _P, _P, _P, _P, _P]
+        L.ref_jk_full.restype = _D
+        L.ref_jk_full.argtypes = [_P, _P, _P, _P, _I]
+        L.ref_jk_screened_sym.restype = _D
+        L.ref_jk_screened_sym.argtypes = [_P, _P, _P, _P, _D]
+        L.ref_eri_quartet.argtypes = [_P, _L, _L, _L, _L, _P]
+        L.ref_schwarz.argtypes = [_P, _P]
+        L.ref_rys.argtypes = [_I, _D, _P, _P]
+        L.ref_boys.argtypes = [_I, _D, _P]
+        L.ref_time_quartets.restype = _D
+        L.ref_time_quartets.argtypes = [_P, _P, _P, _L, _I, _P, _P]
+        L.ref_max_threads.restype = _I
+        _ref = L
+    return _ref
+
+
+# ----------------------------------------------------------------------------
+# Helpers on a libaccint BasisSet-like object (shells with l, center, exps, coefs)
+# ----------------------------------------------------------------------------
+def normalized_arrays(basis):
+    """Flat arrays with coefficients normalized by the restatement (shell.cpp rule)."""
+    O = restatement()
+    l, nprim, centers, exps, coefs, atom = basis.arrays()
+    out = np.zeros_like(coefs)
+    off = 0
+    for s in range(len(l)):
+        k = int(nprim[s])
+        e = np.ascontiguousarray(exps[off:off + k])
+        c = np.ascontiguousarray(coefs[off:off + k])
+        o = np.zeros(k)
+        if basis.prenormalized:
+            o[:] = c
+        else:
+            O.orc_normalize(int(l[s]), k, e.ctypes.data, c.ctypes.data, o.ctypes.data)
+        out[off:off + k] = o
+        off += k
+    return l, nprim, centers, exps, out
+
+
+def orc_jk(basis, D, thr=1e-12):
+    O = restatement()
+    l, nprim, centers, exps, coefs = normalized_arrays(basis)
+    n = basis.nbf
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    J = np.zeros((n, n))
+    K = np.zeros((n, n))
+    nq = O.orc_jk_sym(len(l), l.ctypes.data, nprim.ctypes.data, centers.ctypes.data,
+                      exps.ctypes.data, coefs.ctypes.data, D.ctypes.data, J.ctypes.data,
+                      K.ctypes.data, float(thr))
+    return J, K, nq
+
+
+def orc_quartet(basis, i, j, k, m):
+    O = restatement()
+    l, nprim, centers, exps, coefs = normalized_arrays(basis)
+    nf = [(int(l[x]) + 1) * (int(l[x]) + 2) // 2 for x in (i, j, k, m)]
+    out = np.zeros(int(np.prod(nf)))
+    rc = O.orc_basis_quartet(len(l), l.ctypes.data, nprim.ctypes.data, centers.ctypes.data,
+                             exps.ctypes.data, coefs.ctypes.data, i, j, k, m, out.ctypes.data)
+    assert rc == 0
+    return out.reshape(nf)
+
+
+def orc_schwarz(basis):
+    O = restatement()
+    l, nprim, centers, exps, coefs = normalized_arrays(basis)
+    n = len(l)
+    Q = np.zeros((n, n))
+    O.orc_schwarz(n, l.ctypes.data, nprim.ctypes.data, centers.ctypes.data, exps.ctypes.data,
+                  coefs.ctypes.data, Q.ctypes.data)
+    return Q
+
+
+def orc_rys(n, T):
+    O = restatement()
+    u = np.zeros(n)
+    w = np.zeros(n)
+    O.orc_rys(n, float(T), u.ctypes.data, w.ctypes.data)
+    return u, w
+
+
+def orc_boys(mmax, T):
+    O = restatement()
+    f = np.zeros(mmax + 1)
+    O.orc_boys(mmax, float(T), f.ctypes.data)
+    return f
+
+
+class RefBasis:
+    """A reference BasisSet built from the same shells (reference normalization)."""
+
+    def __init__(self, basis=None, builtin_sto3g=None):
+        R = reference()
+        if R is None:
+            raise RuntimeError("oracle/_ref/libref_oracle.so not built")
+        self.R = R
+        if builtin_sto3g is not None:
+            Z, xyz = builtin_sto3g
+            Z = np.ascontiguousarray(Z, dtype=np.int32)
+            xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+            self.h = R.ref_basis_builtin_sto3g(len(Z), Z.ctypes.data, xyz.ctypes.data)
+        else:
+            l, nprim, centers, exps, coefs, atom = basis.arrays()
+            self._keep = (l, nprim, centers, exps, coefs, atom)
+            self.h = R.ref_basis_create(len(l), l.ctypes.data, nprim.ctypes.data, centers.ctypes.data,
+                                        exps.ctypes.data, coefs.ctypes.data, atom.ctypes.data)
+        if not self.h:
+            raise RuntimeError(R.ref_last_error().decode())
+        self.nbf = R.ref_basis_nbf(self.h)
+        self.nshell = R.ref_basis_nshell(self.h)
+
+    def jk_full(self, D, nthreads=0):
+        n = self.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        J = np.zeros((n, n))
+        K = np.zeros((n, n))
+        t = self.R.ref_jk_full(self.h, D.ctypes.data, J.ctypes.data, K.ctypes.data, nthreads)
+        if t < 0:
+            raise RuntimeError(self.R.ref_last_error().decode())
+        return J, K, t
+
+    def jk_screened(self, D, thr):
+        n = self.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        J = np.zeros((n, n))
+        K = np.zeros((n, n))
+        t = self.R.ref_jk_screened_sym(self.h, D.ctypes.data, J.ctypes.data, K.ctypes.data, float(thr))
+        if t < 0:
+            raise RuntimeError(self.R.ref_last_error().decode())
+        return J, K, t
+
+    def quartet(self, i, j, k, m, shape):
+        out = np.zeros(int(np.prod(shape)))
+        rc = self.R.ref_eri_quartet(self.h, i, j, k, m, out.ctypes.data)
+        assert rc == 0, self.R.ref_last_error().decode()
+        return out.reshape(shape)
+
+    def schwarz(self):
+        Q = np.zeros((self.nshell, self.nshell))
+        self.R.ref_schwarz(self.h, Q.ctypes.data)
+        return Q
+
+    def time_quartets(self, D, quartets, nthreads=0, want_jk=False):
+        n = self.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        q = np.ascontiguousarray(quartets, dtype=np.int64).reshape(-1, 4)
+        J = np.zeros((n, n)) if want_jk else None
+        K = np.zeros((n, n)) if want_jk else None
+        t = self.R.ref_time_quartets(self.h, D.ctypes.data, q.ctypes.data, len(q), nthreads,
+                                     J.ctypes.data if want_jk else None,
+                                     K.ctypes.data if want_jk else None)
+        if t < 0:
+            raise RuntimeError(self.R.ref_last_error().decode())
+        return t, J, K
+
+    def shell_info(self, i):
+        l = ctypes.c_int()
+        k = ctypes.c_int()
+        c = np.zeros(3)
+        fi = ctypes.c_long()
+        self.R.ref_basis_shell(self.h, i, ctypes.byref(l), ctypes.byref(k), c.ctypes.data, None, None,
+                               ctypes.byref(fi))
+        e = np.zeros(k.value)
+        cf = np.zeros(k.value)
+        self.R.ref_basis_shell(self.h, i, ctypes.byref(l), ctypes.byref(k), c.ctypes.data,
+                               e.ctypes.data, cf.ctypes.data, ctypes.byref(fi))
+        return l.value, c, e, cf, fi.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.R.ref_basis_free(self.h)
+            self.h = None

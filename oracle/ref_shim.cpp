@@ -1,0 +1,270 @@
+// Test infrastructure only: a C-ABI shim over the UNMODIFIED reference
+// (LibAccInt) CPU implementation, compiled from the reference's own sources
+// by oracle/Makefile into oracle/_ref/libref_oracle.so.  Only tests/,
+// __graft_entry__.smoke() and bench.py's CPU-baseline/reference arm load it;
+// nothing in the product links it.
+//
+// Every entry point calls the reference's public C++ API:
+//   - Shell(am, center, exps, coefs)          src/shared/basis/shell.cpp:163-187
+//   - BasisSet(shells)                        src/shared/basis/basis_set.cpp:21-29
+//   - data::create_builtin_basis("sto-3g")    src/shared/data/builtin_basis.cpp
+//   - Engine::compute(Operator::coulomb(), FockBuilder)
+//                                             include/libaccint/engine/engine.hpp:435-499,727-731
+//   - Engine::compute_and_consume(op, fb, ScreeningOptions{use_permutation_symmetry})
+//                                             include/libaccint/engine/engine.hpp:1635-1666,1806-1861
+//   - kernels::compute_eri                    src/host/kernels/eri_kernel.cpp:168-381
+//   - screening::SchwarzBounds                src/shared/screening/schwarz_bounds.cpp:16-59
+//   - math::rys_compute / boys_evaluate_array src/shared/math/rys_quadrature.cpp:455-513,
+//                                             src/shared/math/boys_function.cpp:253-303
+//   - FockBuilder::accumulate_symmetric       src/shared/consumers/fock_builder.cpp:123-222
+#include <libaccint/libaccint.hpp>
+#include <libaccint/engine/engine.hpp>
+#include <libaccint/consumers/fock_builder.hpp>
+#include <libaccint/data/builtin_basis.hpp>
+#include <libaccint/kernels/eri_kernel.hpp>
+#include <libaccint/math/rys_quadrature.hpp>
+#include <libaccint/math/boys_function.hpp>
+#include <libaccint/screening/schwarz_bounds.hpp>
+#include <libaccint/screening/screening_options.hpp>
+
+#include <omp.h>
+
+#include <chrono>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <vector>
+
+using namespace libaccint;
+
+namespace {
+
+struct RefBasis {
+    std::unique_ptr<BasisSet> basis;
+};
+
+thread_local char g_err[512] = {0};
+
+void set_err(const char* msg) {
+    std::strncpy(g_err, msg, sizeof(g_err) - 1);
+    g_err[sizeof(g_err) - 1] = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_err; }
+
+// Build a basis from raw (un-normalized) contraction coefficients; the
+// reference Shell constructor applies its own normalization.
+void* ref_basis_create(int nshell, const int* am, const int* nprim,
+                       const double* centers, const double* exps,
+                       const double* coefs, const int* atom_index) {
+    try {
+        std::vector<Shell> shells;
+        shells.reserve(nshell);
+        long off = 0;
+        for (int s = 0; s < nshell; ++s) {
+            std::vector<Real> e(exps + off, exps + off + nprim[s]);
+            std::vector<Real> c(coefs + off, coefs + off + nprim[s]);
+            off += nprim[s];
+            Point3D ctr(centers[3 * s], centers[3 * s + 1], centers[3 * s + 2]);
+            shells.emplace_back(am[s], ctr, std::move(e), std::move(c));
+            if (atom_index) shells.back().set_atom_index(atom_index[s]);
+        }
+        auto* rb = new RefBasis();
+        rb->basis = std::make_unique<BasisSet>(std::move(shells));
+        return rb;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return nullptr;
+    }
+}
+
+void* ref_basis_builtin_sto3g(int natom, const int* Z, const double* xyz) {
+    try {
+        std::vector<data::Atom> atoms;
+        for (int a = 0; a < natom; ++a)
+            atoms.push_back({Z[a], Point3D(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2])});
+        auto* rb = new RefBasis();
+        rb->basis = std::make_unique<BasisSet>(data::create_builtin_basis("sto-3g", atoms));
+        return rb;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return nullptr;
+    }
+}
+
+void ref_basis_free(void* h) { delete static_cast<RefBasis*>(h); }
+
+long ref_basis_nbf(void* h) { return (long)static_cast<RefBasis*>(h)->basis->n_basis_functions(); }
+long ref_basis_nshell(void* h) { return (long)static_cast<RefBasis*>(h)->basis->n_shells(); }
+
+// Export one shell: am, nprim, center, exponents and NORMALIZED coefficients.
+int ref_basis_shell(void* h, long i, int* am, int* nprim, double* center,
+                    double* exps, double* coefs, long* func_index) {
+    const auto& sh = static_cast<RefBasis*>(h)->basis->shell((Size)i);
+    *am = sh.angular_momentum();
+    *nprim = (int)sh.n_primitives();
+    center[0] = sh.center().x;
+    center[1] = sh.center().y;
+    center[2] = sh.center().z;
+    if (exps) for (Size p = 0; p < sh.n_primitives(); ++p) exps[p] = sh.exponents()[p];
+    if (coefs) for (Size p = 0; p < sh.n_primitives(); ++p) coefs[p] = sh.coefficients()[p];
+    *func_index = (long)sh.function_index();
+    return 0;
+}
+
+// Full N^4 race-free OpenMP path: Engine::compute(coulomb, FockBuilder).
+// Returns wall seconds of the compute call, or -1 on error.
+double ref_jk_full(void* h, const double* D, double* J, double* K, int nthreads) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(h)->basis;
+        const Size n = basis.n_basis_functions();
+        if (nthreads > 0) omp_set_num_threads(nthreads);
+        Engine engine(basis);
+        consumers::FockBuilder fb(n);
+        fb.set_density(D, n);
+        auto t0 = std::chrono::steady_clock::now();
+        engine.compute(Operator::coulomb(), fb);
+        auto t1 = std::chrono::steady_clock::now();
+        auto Jm = fb.get_coulomb_matrix();
+        auto Km = fb.get_exchange_matrix();
+        std::memcpy(J, Jm.data(), sizeof(double) * n * n);
+        std::memcpy(K, Km.data(), sizeof(double) * n * n);
+        return std::chrono::duration<double>(t1 - t0).count();
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1.0;
+    }
+}
+
+// Serial Schwarz-screened canonical path with 8-fold symmetric scatter.
+double ref_jk_screened_sym(void* h, const double* D, double* J, double* K, double thr) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(h)->basis;
+        const Size n = basis.n_basis_functions();
+        Engine engine(basis);
+        consumers::FockBuilder fb(n);
+        fb.set_density(D, n);
+        screening::ScreeningOptions opt;
+        opt.threshold = thr;
+        opt.enabled = true;
+        opt.use_permutation_symmetry = true;
+        auto t0 = std::chrono::steady_clock::now();
+        engine.compute_and_consume(Operator::coulomb(), fb, opt);
+        auto t1 = std::chrono::steady_clock::now();
+        auto Jm = fb.get_coulomb_matrix();
+        auto Km = fb.get_exchange_matrix();
+        std::memcpy(J, Jm.data(), sizeof(double) * n * n);
+        std::memcpy(K, Km.data(), sizeof(double) * n * n);
+        return std::chrono::duration<double>(t1 - t0).count();
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1.0;
+    }
+}
+
+// One contracted shell quartet, [a][b][c][d] row-major, norm-corrected Cartesian.
+int ref_eri_quartet(void* h, long i, long j, long k, long l, double* out) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(h)->basis;
+        TwoElectronBuffer<0> buf;
+        kernels::compute_eri(basis.shell(i), basis.shell(j), basis.shell(k), basis.shell(l), buf);
+        const int na = basis.shell(i).n_functions(), nb = basis.shell(j).n_functions();
+        const int nc = basis.shell(k).n_functions(), nd = basis.shell(l).n_functions();
+        long o = 0;
+        for (int a = 0; a < na; ++a)
+            for (int b = 0; b < nb; ++b)
+                for (int c = 0; c < nc; ++c)
+                    for (int d = 0; d < nd; ++d) out[o++] = buf(a, b, c, d);
+        return 0;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1;
+    }
+}
+
+// Schwarz bounds Q_ij (packed upper triangle as the reference stores them).
+int ref_schwarz(void* h, double* Q) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(h)->basis;
+        screening::SchwarzBounds sb(basis);
+        const Size n = basis.n_shells();
+        for (Size i = 0; i < n; ++i)
+            for (Size j = i; j < n; ++j) Q[i * n + j] = Q[j * n + i] = sb(i, j);
+        return 0;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1;
+    }
+}
+
+void ref_rys(int n, double T, double* roots, double* weights) {
+    math::rys_compute(n, T, roots, weights);
+}
+
+void ref_boys(int mmax, double T, double* out) { math::boys_evaluate_array(mmax, T, out); }
+
+// Time a caller-supplied list of canonical shell quartets through the
+// reference's compute_2e_shell_quartet + FockBuilder::accumulate_symmetric,
+// on nthreads OpenMP threads with one FockBuilder per thread (race-free),
+// reduced into J/K at the end.  Returns wall seconds of the parallel region.
+double ref_time_quartets(void* h, const double* D, const long* quartets, long nq,
+                         int nthreads, double* J, double* K) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(h)->basis;
+        const Size n = basis.n_basis_functions();
+        if (nthreads <= 0) nthreads = omp_get_max_threads();
+        std::vector<std::unique_ptr<consumers::FockBuilder>> fbs(nthreads);
+        for (int t = 0; t < nthreads; ++t) {
+            fbs[t] = std::make_unique<consumers::FockBuilder>(n);
+            fbs[t]->set_density(D, n);
+        }
+        Engine engine(basis);
+        auto& cpu = engine.cpu_engine();
+        const Operator op = Operator::coulomb();
+        auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel num_threads(nthreads)
+        {
+            TwoElectronBuffer<0> buf;
+            auto& fb = *fbs[omp_get_thread_num()];
+#pragma omp for schedule(dynamic, 8)
+            for (long q = 0; q < nq; ++q) {
+                const long i = quartets[4 * q], j = quartets[4 * q + 1];
+                const long k = quartets[4 * q + 2], l = quartets[4 * q + 3];
+                const auto& a = basis.shell(i);
+                const auto& b = basis.shell(j);
+                const auto& c = basis.shell(k);
+                const auto& d = basis.shell(l);
+                cpu.compute_2e_shell_quartet(op, a, b, c, d, buf);
+                fb.accumulate_symmetric(buf, a.function_index(), b.function_index(),
+                                        c.function_index(), d.function_index(),
+                                        a.n_functions(), b.n_functions(), c.n_functions(),
+                                        d.n_functions(), i == j, k == l, (i == k && j == l));
+            }
+        }
+        auto t1 = std::chrono::steady_clock::now();
+        if (J && K) {
+            std::memset(J, 0, sizeof(double) * n * n);
+            std::memset(K, 0, sizeof(double) * n * n);
+            for (int t = 0; t < nthreads; ++t) {
+                auto Jm = fbs[t]->get_coulomb_matrix();
+                auto Km = fbs[t]->get_exchange_matrix();
+                for (Size x = 0; x < n * n; ++x) {
+                    J[x] += Jm[x];
+                    K[x] += Km[x];
+                }
+            }
+        }
+        return std::chrono::duration<double>(t1 - t0).count();
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1.0;
+    }
+}
+
+int ref_max_threads() { return omp_get_max_threads(); }
+
+}  // extern "C"

@@ -1,0 +1,456 @@
+/*
+ * Test infrastructure only -- the CPU ORACLE for the J/K hot path.
+ *
+ * A plain-C restatement of the reference (LibAccInt v0.1.0-alpha.2) algorithm
+ * for Rys-quadrature ERIs over contracted Cartesian Gaussians and their 8-fold
+ * symmetric digestion into J and K.  Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg may load this library; the product never does.
+ *
+ * Precision: Boys moments and Rys roots/weights are computed in IEEE binary128
+ * (__float128, libquadmath) and rounded to double; everything downstream runs in
+ * double like the reference.  That makes the roots independent of (and more
+ * accurate than) both the reference's FP64 Chebyshev+QL+Newton path and the
+ * CUDA path's fitted tables, so the oracle can arbitrate between them.
+ *
+ * Functions and the reference code each one restates:
+ *   orc_boys           src/shared/math/boys_function.cpp:253-303 (F_0..F_m(T));
+ *                      here: positive series for T<=50, erf + upward recursion above.
+ *   orc_rys            src/shared/math/rys_quadrature.cpp:455-513 (rys_compute):
+ *                      moments F_k(T) -> recurrence coefficients (Chebyshev
+ *                      algorithm on ordinary moments, in binary128 instead of the
+ *                      reference's modified moments in double, :24-66) -> roots as
+ *                      eigenvalues of the Jacobi matrix (Sturm bisection in x87
+ *                      extended precision, then binary128 Newton on the
+ *                      characteristic polynomial, instead of implicit QL, :75-157)
+ *                      -> Christoffel weights.
+ *                      Roots clamped to [1e-14, 1-1e-14] as at :497-500.
+ *   orc_normalize      src/shared/basis/shell.cpp:32-113 (primitive normalization
+ *                      and (l,0,0) self-overlap rescaling).
+ *   orc_eri_quartet    src/host/kernels/eri_kernel.cpp:104-164 (build_2d_rys: VRR on
+ *                      a then c, HRR to b then d) and :168-381 (primitive loops,
+ *                      prefactor 2 pi^{5/2}/(zeta eta sqrt(zeta+eta)) K_AB K_CD,
+ *                      assembly, norm_correction of
+ *                      include/libaccint/kernels/norm_correction.hpp:28-34).
+ *   orc_schwarz        src/shared/screening/schwarz_bounds.cpp:20-59.
+ *   orc_jk_sym         include/libaccint/engine/engine.hpp:1806-1861 (canonical
+ *                      i<=j, k>=i, l>=(k==i?j:k) loop with Schwarz test) and
+ *                      src/shared/consumers/fock_builder.cpp:123-222
+ *                      (accumulate_symmetric: 8 permutations with degeneracy flags).
+ *
+ * Cartesian order inside a shell: lx descending, then ly descending
+ * (include/libaccint/math/cartesian_indices.hpp:26-36).
+ */
+#include <math.h>
+#include <quadmath.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef __float128 q_t;
+
+#define ORC_MAX_L 6           /* shells up to l=6 (gradient tests shift l by +1) */
+#define ORC_MAX_ROOTS 13
+#define ORC_MAX_MOM (2 * ORC_MAX_ROOTS)
+
+/* ------------------------------------------------------------------------- */
+/* Boys function F_m(T) = int_0^1 t^{2m} exp(-T t^2) dt, binary128.           */
+/* ------------------------------------------------------------------------- */
+static void boys_q(int mmax, q_t T, q_t *F) {
+    if (T <= 50) {
+        /* F_m(T) = exp(-T) sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)); all terms
+           positive, so no cancellation.  Evaluate at mmax, recurse downward. */
+        q_t term = 1.0Q / (2 * mmax + 1), sum = term;
+        for (int k = 1; k < 2000; ++k) {
+            term *= 2 * T / (2 * mmax + 2 * k + 1);
+            sum += term;
+            if (term < 1e-38Q * sum) break;
+        }
+        q_t e = expq(-T);
+        F[mmax] = e * sum;
+        for (int m = mmax; m >= 1; --m) F[m - 1] = (2 * T * F[m] + e) / (2 * m - 1);
+    } else {
+        /* upward recursion is stable while (2m+1)/(2T) < 1, true for m <= 2*13 */
+        q_t e = expq(-T);
+        F[0] = 0.5Q * sqrtq(M_PIq / T) * erfq(sqrtq(T));
+        for (int m = 0; m < mmax; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2 * T);
+    }
+}
+
+void orc_boys(int mmax, double T, double *out) {
+    q_t F[64];
+    if (mmax > 63) mmax = 63;
+    boys_q(mmax, (q_t)T, F);
+    for (int m = 0; m <= mmax; ++m) out[m] = (double)F[m];
+}
+
+/* ------------------------------------------------------------------------- */
+/* Rys roots and weights in binary128.                                        */
+/* Measure: d mu(u) on [0,1] with moments mu_k = F_k(T) (u = t^2).            */
+/* ------------------------------------------------------------------------- */
+static void chebyshev_recurrence(int n, const q_t *mu, q_t *alpha, q_t *beta) {
+    /* Chebyshev algorithm on ordinary moments (Gautschi's sigma table). */
+    q_t sig_prev[ORC_MAX_MOM + 2], sig[ORC_MAX_MOM + 2], sig_new[ORC_MAX_MOM + 2];
+    const int nm = 2 * n;
+    for (int l = 0; l < nm; ++l) { sig_prev[l] = 0; sig[l] = mu[l]; }
+    alpha[0] = mu[1] / mu[0];
+    beta[0] = mu[0];
+    for (int k = 1; k < n; ++k) {
+        for (int l = k; l < nm - k; ++l)
+            sig_new[l] = sig[l + 1] - alpha[k - 1] * sig[l] - beta[k - 1] * sig_prev[l];
+        alpha[k] = sig_new[k + 1] / sig_new[k] - sig[k] / sig[k - 1];
+        beta[k] = sig_new[k] / sig[k - 1];
+        for (int l = 0; l < nm; ++l) { sig_prev[l] = sig[l]; sig[l] = sig_new[l]; }
+    }
+}
+
+/* Monic orthogonal polynomial p_n(x) and derivative via the recurrence. */
+static void charpoly(int n, const q_t *a, const q_t *b, q_t x, q_t *p, q_t *dp) {
+    q_t pm1 = 0, p0 = 1, dpm1 = 0, dp0 = 0;
+    for (int k = 0; k < n; ++k) {
+        q_t p1 = (x - a[k]) * p0 - (k ? b[k] * pm1 : 0);
+        q_t dp1 = p0 + (x - a[k]) * dp0 - (k ? b[k] * dpm1 : 0);
+        pm1 = p0; p0 = p1; dpm1 = dp0; dp0 = dp1;
+    }
+    *p = p0;
+    *dp = dp0;
+}
+
+static int sturm_count_ld(int n, const long double *a, const long double *b, long double x) {
+    int cnt = 0;
+    long double d = a[0] - x;
+    if (d < 0) cnt++;
+    for (int k = 1; k < n; ++k) {
+        if (d == 0) d = 1e-4000L;
+        d = a[k] - x - b[k] / d;
+        if (d < 0) cnt++;
+    }
+    return cnt;
+}
+
+static void rys_q(int n, q_t T, q_t *roots, q_t *weights) {
+    q_t mu[ORC_MAX_MOM + 2], a[ORC_MAX_ROOTS], b[ORC_MAX_ROOTS];
+    long double al[ORC_MAX_ROOTS], bl[ORC_MAX_ROOTS];
+    boys_q(2 * n - 1, T, mu);
+    chebyshev_recurrence(n, mu, a, b);
+    for (int k = 0; k < n; ++k) { al[k] = (long double)a[k]; bl[k] = (long double)b[k]; }
+    for (int r = 0; r < n; ++r) {
+        /* r-th smallest eigenvalue: Sturm bisection in extended precision to
+           bracket it, then Newton on the binary128 characteristic polynomial. */
+        long double lo = 0, hi = 1;
+        for (int it = 0; it < 64; ++it) {
+            long double mid = 0.5L * (lo + hi);
+            if (sturm_count_ld(n, al, bl, mid) > r) hi = mid; else lo = mid;
+        }
+        q_t x = 0.5Q * ((q_t)lo + (q_t)hi);
+        for (int it = 0; it < 4; ++it) {
+            q_t p, dp;
+            charpoly(n, a, b, x, &p, &dp);
+            if (dp == 0) break;
+            x = x - p / dp;
+        }
+        roots[r] = x;
+        /* Christoffel number: w = 1 / sum_k P_k(x)^2 with orthonormal P_k. */
+        q_t pm1 = 0, p0 = 1 / sqrtq(b[0]), s = p0 * p0;
+        for (int k = 0; k + 1 < n; ++k) {
+            q_t p1 = ((x - a[k]) * p0 - (k ? sqrtq(b[k]) * pm1 : 0)) / sqrtq(b[k + 1]);
+            s += p1 * p1;
+            pm1 = p0; p0 = p1;
+        }
+        weights[r] = 1 / s;
+    }
+}
+
+void orc_rys(int n, double T, double *roots, double *weights) {
+    q_t r[ORC_MAX_ROOTS], w[ORC_MAX_ROOTS];
+    rys_q(n, (q_t)T, r, w);
+    for (int i = 0; i < n; ++i) {
+        double u = (double)r[i];
+        if (u < 1e-14) u = 1e-14;
+        if (u > 1.0 - 1e-14) u = 1.0 - 1e-14;
+        roots[i] = u;
+        weights[i] = (double)w[i];
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Shell normalization (PySCF cart convention, unit (l,0,0) self-overlap).   */
+/* ------------------------------------------------------------------------- */
+static double dfact_odd(int l) { /* (2l-1)!! */
+    double r = 1;
+    for (int k = 2 * l - 1; k > 1; k -= 2) r *= k;
+    return r;
+}
+
+void orc_normalize(int l, int nprim, const double *exps, const double *coefs, double *out) {
+    for (int p = 0; p < nprim; ++p)
+        out[p] = coefs[p] * pow(2 * exps[p] / M_PI, 0.75) * pow(4 * exps[p], 0.5 * l) /
+                 sqrt(dfact_odd(l));
+    double s = 0;
+    for (int p = 0; p < nprim; ++p)
+        for (int q = 0; q < nprim; ++q) {
+            double z = exps[p] + exps[q];
+            double ov = pow(M_PI / z, 1.5);
+            for (int k = 0; k < l; ++k) ov *= 0.5 / z;
+            s += out[p] * out[q] * ov;
+        }
+    double sc = 1 / sqrt(s);
+    for (int p = 0; p < nprim; ++p) out[p] *= sc;
+}
+
+/* ------------------------------------------------------------------------- */
+/* One contracted shell quartet (ab|cd), out[a][b][c][d] row-major.           */
+/* ------------------------------------------------------------------------- */
+static int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+static void cart_list(int l, int (*c)[3]) {
+    int k = 0;
+    for (int x = l; x >= 0; --x)
+        for (int y = l - x; y >= 0; --y) { c[k][0] = x; c[k][1] = y; c[k][2] = l - x - y; ++k; }
+}
+
+/* 2D table I[a][b][c][d] for one direction and one root. */
+static void table2d(int la, int lb, int lc, int ld, double pa, double qc, double ab, double cd,
+                    double b10, double b01, double b00, double *I) {
+    const int da = la + lb + 1, db = lb + 1, dc = lc + ld + 1, dd = ld + 1;
+#define IX(a, b, c, d) I[(((a) * db + (b)) * dc + (c)) * dd + (d)]
+    memset(I, 0, sizeof(double) * da * db * dc * dd);
+    IX(0, 0, 0, 0) = 1.0;
+    for (int a = 0; a < la + lb; ++a)
+        IX(a + 1, 0, 0, 0) = pa * IX(a, 0, 0, 0) + (a ? a * b10 * IX(a - 1, 0, 0, 0) : 0.0);
+    for (int c = 0; c < lc + ld; ++c)
+        for (int a = 0; a <= la + lb; ++a)
+            IX(a, 0, c + 1, 0) = qc * IX(a, 0, c, 0) + (c ? c * b01 * IX(a, 0, c - 1, 0) : 0.0) +
+                                 (a ? a * b00 * IX(a - 1, 0, c, 0) : 0.0);
+    for (int b = 0; b < lb; ++b)
+        for (int a = 0; a <= la + lb - b - 1; ++a)
+            for (int c = 0; c <= lc + ld; ++c)
+                IX(a, b + 1, c, 0) = IX(a + 1, b, c, 0) + ab * IX(a, b, c, 0);
+    for (int d = 0; d < ld; ++d)
+        for (int a = 0; a <= la; ++a)
+            for (int b = 0; b <= lb; ++b)
+                for (int c = 0; c <= lc + ld - d - 1; ++c)
+                    IX(a, b, c, d + 1) = IX(a, b, c + 1, d) + cd * IX(a, b, c, d);
+#undef IX
+}
+
+/* Shell descriptors: l[4], centers[4][3], nprim[4], exps/coefs (normalized). */
+int orc_eri_quartet(const int *l, const double *ctr, const int *nprim, const double *const *exps,
+                    const double *const *coefs, double *out) {
+    const int la = l[0], lb = l[1], lc = l[2], ld = l[3];
+    if (la > ORC_MAX_L || lb > ORC_MAX_L || lc > ORC_MAX_L || ld > ORC_MAX_L) return -1;
+    const double *A = ctr, *B = ctr + 3, *C = ctr + 6, *D = ctr + 9;
+    const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
+    int ca[28][3], cb[28][3], cc[28][3], cdl[28][3];
+    cart_list(la, ca); cart_list(lb, cb); cart_list(lc, cc); cart_list(ld, cdl);
+    const int nroots = (la + lb + lc + ld) / 2 + 1;
+    const int da = la + lb + 1, db = lb + 1, dc = lc + ld + 1, dd = ld + 1;
+    const int tsz = da * db * dc * dd;
+    double *Ix = malloc(sizeof(double) * tsz * 3), *Iy = Ix + tsz, *Iz = Iy + tsz;
+    const long nout = (long)na * nb * nc * nd;
+    memset(out, 0, sizeof(double) * nout);
+    const double pi52 = M_PI * M_PI * sqrt(M_PI);
+    double AB[3], CD[3];
+    for (int x = 0; x < 3; ++x) { AB[x] = A[x] - B[x]; CD[x] = C[x] - D[x]; }
+    double roots[ORC_MAX_ROOTS], wts[ORC_MAX_ROOTS];
+#define TI(T, a, b, c, d) T[(((a) * db + (b)) * dc + (c)) * dd + (d)]
+    for (int p = 0; p < nprim[0]; ++p)
+        for (int q = 0; q < nprim[1]; ++q) {
+            const double al = exps[0][p], be = exps[1][q];
+            const double zeta = al + be;
+            double P[3], ab2 = 0;
+            for (int x = 0; x < 3; ++x) { P[x] = (al * A[x] + be * B[x]) / zeta; ab2 += AB[x] * AB[x]; }
+            const double Kab = exp(-al * be / zeta * ab2);
+            for (int r = 0; r < nprim[2]; ++r)
+                for (int s = 0; s < nprim[3]; ++s) {
+                    const double ga = exps[2][r], de = exps[3][s];
+                    const double eta = ga + de;
+                    double Q[3], cd2 = 0, PQ[3], pq2 = 0;
+                    for (int x = 0; x < 3; ++x) {
+                        Q[x] = (ga * C[x] + de * D[x]) / eta;
+                        cd2 += CD[x] * CD[x];
+                        PQ[x] = P[x] - Q[x];
+                        pq2 += PQ[x] * PQ[x];
+                    }
+                    const double Kcd = exp(-ga * de / eta * cd2);
+                    const double rho = zeta * eta / (zeta + eta);
+                    const double T = rho * pq2;
+                    const double pref = 2.0 * pi52 / (zeta * eta * sqrt(zeta + eta)) * Kab * Kcd;
+                    const double coef = coefs[0][p] * coefs[1][q] * coefs[2][r] * coefs[3][s] * pref;
+                    orc_rys(nroots, T, roots, wts);
+                    for (int k = 0; k < nroots; ++k) {
+                        const double u = roots[k];
+                        const double b10 = 0.5 / zeta * (1.0 - rho / zeta * u);
+                        const double b01 = 0.5 / eta * (1.0 - rho / eta * u);
+                        const double b00 = 0.5 / (zeta + eta) * u;
+                        double *T3[3] = {Ix, Iy, Iz};
+                        for (int x = 0; x < 3; ++x) {
+                            const double pa = (P[x] - A[x]) - rho / zeta * u * PQ[x];
+                            const double qc = (Q[x] - C[x]) + rho / eta * u * PQ[x];
+                            table2d(la, lb, lc, ld, pa, qc, AB[x], CD[x], b10, b01, b00, T3[x]);
+                        }
+                        const double wc = coef * wts[k];
+                        long o = 0;
+                        for (int ia = 0; ia < na; ++ia)
+                            for (int ib = 0; ib < nb; ++ib)
+                                for (int ic = 0; ic < nc; ++ic)
+                                    for (int id = 0; id < nd; ++id, ++o)
+                                        out[o] += wc *
+                                            TI(Ix, ca[ia][0], cb[ib][0], cc[ic][0], cdl[id][0]) *
+                                            TI(Iy, ca[ia][1], cb[ib][1], cc[ic][1], cdl[id][1]) *
+                                            TI(Iz, ca[ia][2], cb[ib][2], cc[ic][2], cdl[id][2]);
+                    }
+                }
+        }
+#undef TI
+    long o = 0;
+    for (int ia = 0; ia < na; ++ia)
+        for (int ib = 0; ib < nb; ++ib)
+            for (int ic = 0; ic < nc; ++ic)
+                for (int id = 0; id < nd; ++id, ++o) {
+                    double den = dfact_odd(ca[ia][0]) * dfact_odd(ca[ia][1]) * dfact_odd(ca[ia][2]) *
+                                 dfact_odd(cb[ib][0]) * dfact_odd(cb[ib][1]) * dfact_odd(cb[ib][2]) *
+                                 dfact_odd(cc[ic][0]) * dfact_odd(cc[ic][1]) * dfact_odd(cc[ic][2]) *
+                                 dfact_odd(cdl[id][0]) * dfact_odd(cdl[id][1]) * dfact_odd(cdl[id][2]);
+                    out[o] /= sqrt(den);
+                }
+    free(Ix);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Basis-level helpers: shells given as flat arrays, coefficients normalized. */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int n;
+    const int *l, *nprim;
+    const double *ctr, *exps, *coefs;
+    long *poff, *foff;
+} basis_t;
+
+static void basis_init(basis_t *b, int n, const int *l, const int *nprim, const double *ctr,
+                       const double *exps, const double *coefs) {
+    b->n = n; b->l = l; b->nprim = nprim; b->ctr = ctr; b->exps = exps; b->coefs = coefs;
+    b->poff = malloc(sizeof(long) * (n + 1));
+    b->foff = malloc(sizeof(long) * (n + 1));
+    b->poff[0] = b->foff[0] = 0;
+    for (int s = 0; s < n; ++s) {
+        b->poff[s + 1] = b->poff[s] + nprim[s];
+        b->foff[s + 1] = b->foff[s] + ncart(l[s]);
+    }
+}
+
+static void basis_free(basis_t *b) { free(b->poff); free(b->foff); }
+
+static int quartet(const basis_t *b, int i, int j, int k, int m, double *out) {
+    int l[4] = {b->l[i], b->l[j], b->l[k], b->l[m]};
+    int np[4] = {b->nprim[i], b->nprim[j], b->nprim[k], b->nprim[m]};
+    double ctr[12];
+    memcpy(ctr, b->ctr + 3 * i, 24); memcpy(ctr + 3, b->ctr + 3 * j, 24);
+    memcpy(ctr + 6, b->ctr + 3 * k, 24); memcpy(ctr + 9, b->ctr + 3 * m, 24);
+    const double *e[4] = {b->exps + b->poff[i], b->exps + b->poff[j], b->exps + b->poff[k],
+                          b->exps + b->poff[m]};
+    const double *c[4] = {b->coefs + b->poff[i], b->coefs + b->poff[j], b->coefs + b->poff[k],
+                          b->coefs + b->poff[m]};
+    return orc_eri_quartet(l, ctr, np, e, c, out);
+}
+
+/* One contracted quartet of a basis by shell indices. */
+int orc_basis_quartet(int n, const int *l, const int *nprim, const double *ctr, const double *exps,
+                      const double *coefs, int i, int j, int k, int m, double *out) {
+    basis_t b;
+    basis_init(&b, n, l, nprim, ctr, exps, coefs);
+    int rc = quartet(&b, i, j, k, m, out);
+    basis_free(&b);
+    return rc;
+}
+
+/* Schwarz bounds Q[i*n+j] = sqrt(max_ab |(ab|ab)|). */
+int orc_schwarz(int n, const int *l, const int *nprim, const double *ctr, const double *exps,
+                const double *coefs, double *Q) {
+    basis_t b;
+    basis_init(&b, n, l, nprim, ctr, exps, coefs);
+    double *buf = malloc(sizeof(double) * 28 * 28 * 28 * 28);
+    for (int i = 0; i < n; ++i)
+        for (int j = i; j < n; ++j) {
+            quartet(&b, i, j, i, j, buf);
+            const int ni = ncart(l[i]), nj = ncart(l[j]);
+            double mx = 0;
+            for (int a = 0; a < ni; ++a)
+                for (int c = 0; c < nj; ++c) {
+                    double v = fabs(buf[((long)(a * nj + c) * ni + a) * nj + c]);
+                    if (v > mx) mx = v;
+                }
+            Q[i * n + j] = Q[j * n + i] = sqrt(mx);
+        }
+    free(buf);
+    basis_free(&b);
+    return 0;
+}
+
+/* Canonical screened loop + 8-fold symmetric scatter (serial).  D symmetric,
+   row-major nbf x nbf; J and K are overwritten.  Returns the number of
+   canonical quartets computed. */
+long orc_jk_sym(int n, const int *l, const int *nprim, const double *ctr, const double *exps,
+                const double *coefs, const double *D, double *J, double *K, double thr) {
+    basis_t b;
+    basis_init(&b, n, l, nprim, ctr, exps, coefs);
+    const long nbf = b.foff[n];
+    double *Q = malloc(sizeof(double) * n * n);
+    orc_schwarz(n, l, nprim, ctr, exps, coefs, Q);
+    double *g = malloc(sizeof(double) * 28 * 28 * 28 * 28);
+    memset(J, 0, sizeof(double) * nbf * nbf);
+    memset(K, 0, sizeof(double) * nbf * nbf);
+    long count = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j = i; j < n; ++j)
+            for (int k = i; k < n; ++k)
+                for (int m = (k == i ? j : k); m < n; ++m) {
+                    if (Q[i * n + j] * Q[k * n + m] < thr) continue;
+                    quartet(&b, i, j, k, m, g);
+                    ++count;
+                    const int ij = (i == j), kl = (k == m), bk = (i == k && j == m);
+                    const int na = ncart(l[i]), nb = ncart(l[j]), nc = ncart(l[k]), nd = ncart(l[m]);
+                    long o = 0;
+                    for (int a = 0; a < na; ++a)
+                        for (int bb = 0; bb < nb; ++bb)
+                            for (int c = 0; c < nc; ++c)
+                                for (int d = 0; d < nd; ++d, ++o) {
+                                    const long mu = b.foff[i] + a, nu = b.foff[j] + bb;
+                                    const long la = b.foff[k] + c, si = b.foff[m] + d;
+                                    const double v = g[o];
+                                    J[mu * nbf + nu] += v * D[la * nbf + si];
+                                    K[mu * nbf + la] += v * D[nu * nbf + si];
+                                    if (!kl) {
+                                        J[mu * nbf + nu] += v * D[si * nbf + la];
+                                        K[mu * nbf + si] += v * D[nu * nbf + la];
+                                    }
+                                    if (!ij) {
+                                        J[nu * nbf + mu] += v * D[la * nbf + si];
+                                        K[nu * nbf + la] += v * D[mu * nbf + si];
+                                    }
+                                    if (!ij && !kl) {
+                                        J[nu * nbf + mu] += v * D[si * nbf + la];
+                                        K[nu * nbf + si] += v * D[mu * nbf + la];
+                                    }
+                                    if (!bk) {
+                                        J[la * nbf + si] += v * D[mu * nbf + nu];
+                                        K[la * nbf + mu] += v * D[nu * nbf + si];
+                                        if (!ij) {
+                                            J[la * nbf + si] += v * D[nu * nbf + mu];
+                                            K[la * nbf + nu] += v * D[mu * nbf + si];
+                                        }
+                                        if (!kl) {
+                                            J[si * nbf + la] += v * D[mu * nbf + nu];
+                                            K[si * nbf + mu] += v * D[nu * nbf + la];
+                                        }
+                                        if (!ij && !kl) {
+                                            J[si * nbf + la] += v * D[nu * nbf + mu];
+                                            K[si * nbf + nu] += v * D[mu * nbf + la];
+                                        }
+                                    }
+                                }
+                }
+    free(g);
+    free(Q);
+    basis_free(&b);
+    return count;
+}
