@@ -107,6 +107,11 @@ typedef struct {
   double fp32_cut;   /* mixed precision: quartets with Q_ij*Q_kl*max|D| < fp32_cut
                         run the Rys recursion in FP32 (0 = all FP64)             */
   int check_symmetric; /* 1 = reject a D that is not symmetric to 1e-12 (host)  */
+  int shard_index;     /* multi-GPU: this rank computes shard shard_index of     */
+  int shard_count;     /* shard_count equal slices of every quartet block (1 = all);
+                          J/K then hold this rank's partial sums -- add them over
+                          ranks (one all-reduce) to get the full J/K            */
+  int profile;         /* 1 = time every kernel launch (lai_jk_last_profile)    */
 } lai_jk_opts;
 LAI_API void lai_jk_opts_default(lai_jk_opts* opts);
 
@@ -146,6 +151,26 @@ typedef struct {
 LAI_API int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_capacity,
                                    lai_quartet_meta* meta, size_t meta_capacity,
                                    int64_t* n_quartets, int64_t* n_values);
+
+/* ---------------------------------------------------------------------------
+ * Measurement helpers (no counterpart in the reference, which has no device
+ * profiling of this path).
+ * ------------------------------------------------------------------------- */
+/* Per-launch device times of the last build made with opts.profile = 1.  For
+ * launch i: ms[i], algorithmic FLOP alg_flops[i], quartets[i], class
+ * (la,lb,lc,ld) in lclass[4*i..4*i+3].  Returns the launch count, or < 0. */
+LAI_API int lai_jk_last_profile(lai_engine* engine, int capacity, double* ms, double* alg_flops,
+                                int64_t* quartets, int* lclass);
+/* n canonical screened quartets drawn uniformly (seeded) from all of the
+ * engine's quartets, as shell indices [n][4] in the order the engine computes
+ * them.  Used to time the reference CPU path on a bounded sample. */
+LAI_API int lai_engine_sample_quartets(lai_engine* engine, int64_t n, uint64_t seed,
+                                       int32_t* quartets);
+/* Total canonical screened quartets of the engine. */
+LAI_API int64_t lai_engine_quartet_count(lai_engine* engine);
+/* FP64 FMA throughput of the device measured by a register-resident FMA loop
+ * (TFLOP/s, 2 FLOP per FMA): the speed-of-light denominator of the FP64 path. */
+LAI_API int lai_probe_fp64_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }

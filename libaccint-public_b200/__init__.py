@@ -5,5 +5,5 @@ directory name is not a Python identifier).
 """
 from ._lib import LibAccIntError, lib  # noqa: F401
 from .basis import BasisSet, Shell, basis_data  # noqa: F401
-from .engine import Engine, FockBuilder, Operator, ScreeningOptions, jk  # noqa: F401
+from .engine import Engine, FockBuilder, Operator, ScreeningOptions, jk, probe_fp64_peak  # noqa: F401
 from . import molecules, workloads  # noqa: F401

@@ -19,6 +19,8 @@ EXPORTED = [
     "lai_basis_create", "lai_basis_destroy", "lai_basis_nbf", "lai_basis_nshell", "lai_basis_shell",
     "lai_engine_opts_default", "lai_engine_create", "lai_engine_destroy", "lai_engine_schwarz",
     "lai_jk_opts_default", "lai_jk_build", "lai_jk_build_device", "lai_eri_batch_screened",
+    "lai_jk_last_profile", "lai_engine_sample_quartets", "lai_engine_quartet_count",
+    "lai_probe_fp64_peak",
 ]
 
 
@@ -33,7 +35,8 @@ class EngineOpts(ctypes.Structure):
 
 
 class JKOpts(ctypes.Structure):
-    _fields_ = [("fp32_cut", ctypes.c_double), ("check_symmetric", ctypes.c_int)]
+    _fields_ = [("fp32_cut", ctypes.c_double), ("check_symmetric", ctypes.c_int),
+                ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int), ("profile", ctypes.c_int)]
 
 
 class QuartetMeta(ctypes.Structure):
@@ -77,6 +80,10 @@ def lib():
         "lai_jk_build_device": (I, [P, P, P, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKReport)]),
         "lai_eri_batch_screened": (I, [P, P, ctypes.c_size_t, P, ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+        "lai_jk_last_profile": (I, [P, I, P, P, P, P]),
+        "lai_engine_sample_quartets": (I, [P, ctypes.c_int64, ctypes.c_uint64, P]),
+        "lai_engine_quartet_count": (ctypes.c_int64, [P]),
+        "lai_probe_fp64_peak": (I, [I, ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

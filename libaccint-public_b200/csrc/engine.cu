@@ -260,7 +260,13 @@ struct lai_engine {
   size_t scratch_doubles = 0;
   DevBuf d_status;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-launch profile of the last build with opts.profile
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<int> prof_block;
+  std::vector<int64_t> prof_quartets;
+  int prof_n = 0;
   ~lai_engine() {
+    for (auto e : prof_ev) cudaEventDestroy(e);
     classes.clear();
     blocks.clear();
     if (ev0) cudaEventDestroy(ev0);
@@ -365,8 +371,14 @@ int ensure_scratch(lai_engine* E, size_t doubles) {
 int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs& args) {
   const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
   if (lai::small_class_supported(la, lb, lc, ld)) {
-    const int rc = lai::launch_small(blk, args, E->tab, E->stream, false);
+    const int rc = lai::launch_small(blk, args, E->tab, E->stream, false, E->num_sms);
     if (rc < 0) return fail(LAI_ECUDA, std::string("small-class launch failed: ") +
+                                           cudaGetErrorString(cudaGetLastError()));
+    return LAI_OK;
+  }
+  if (lai::sliced_class_supported(la, lb, lc, ld)) {
+    const int rc = lai::launch_sliced(blk, args, E->tab, E->stream, false, E->num_sms);
+    if (rc < 0) return fail(LAI_ECUDA, std::string("sliced launch failed: ") +
                                            cudaGetErrorString(cudaGetLastError()));
     return LAI_OK;
   }
@@ -489,9 +501,11 @@ lai::QuartetBlock make_block(const lai_engine* E, const ClassPairBlock& b) {
 }
 
 int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t stream,
-           lai_jk_report* rep, bool timed) {
+           const lai_jk_opts& o, lai_jk_report* rep, bool timed) {
   const int nbf = (int)E->basis->nbf;
   const size_t bytes = sizeof(double) * (size_t)nbf * nbf;
+  if (o.shard_count < 1 || o.shard_index < 0 || o.shard_index >= o.shard_count)
+    return fail(LAI_EINVAL, "lai_jk: bad shard_index/shard_count");
   if (E->d_Jp.bytes < bytes) {
     LAI_CUDA_TRY(E->d_Jp.alloc(bytes));
     LAI_CUDA_TRY(E->d_Kp.alloc(bytes));
@@ -510,12 +524,37 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
   int launches = 0;
   int64_t nq = 0;
   double flops = 0;
-  for (auto& bp : E->blocks) {
-    const lai::QuartetBlock q = make_block(E, *bp);
+  if (o.profile) {
+    const size_t need = 2 * E->blocks.size();
+    while (E->prof_ev.size() < need) {
+      cudaEvent_t ev;
+      LAI_CUDA_TRY(cudaEventCreate(&ev));
+      E->prof_ev.push_back(ev);
+    }
+    E->prof_block.clear();
+    E->prof_quartets.clear();
+  }
+  E->prof_n = 0;
+  for (size_t b = 0; b < E->blocks.size(); ++b) {
+    const auto& bp = *E->blocks[b];
+    lai::QuartetBlock q = make_block(E, bp);
+    // this shard's contiguous slice of the block
+    const int64_t lo = bp.total * o.shard_index / o.shard_count;
+    const int64_t hi = bp.total * (o.shard_index + 1) / o.shard_count;
+    if (hi <= lo) continue;
+    q.t_begin = lo;
+    q.total = hi;
+    if (o.profile) LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n], stream));
     if (int rc = launch_block(E, q, args)) { E->stream = saved; return rc; }
+    if (o.profile) {
+      LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n + 1], stream));
+      E->prof_block.push_back((int)b);
+      E->prof_quartets.push_back(hi - lo);
+      ++E->prof_n;
+    }
     ++launches;
-    nq += bp->total;
-    flops += bp->alg_flops * (double)bp->total;
+    nq += hi - lo;
+    flops += bp.alg_flops * (double)(hi - lo);
   }
   const int64_t nn = (int64_t)nbf * nbf;
   if (nn > 0) {
@@ -536,6 +575,29 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
   return LAI_OK;
 }
 
+// splitmix64
+inline uint64_t mix64(uint64_t& x) {
+  uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void fp64_fma_probe(double* out, int iters) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-10, a2 = a0 + 2e-10, a3 = a0 + 3e-10;
+  double a4 = a0 + 4e-10, a5 = a0 + 5e-10, a6 = a0 + 6e-10, a7 = a0 + 7e-10;
+  const double m = 0.999999, c = 1e-7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+      a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+    }
+  }
+  const double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (r == 12345.678) out[0] = r;  // keep the chain alive
+}
+
 }  // namespace
 
 extern "C" {
@@ -550,6 +612,9 @@ void lai_jk_opts_default(lai_jk_opts* opts) {
   if (!opts) return;
   opts->fp32_cut = 0.0;
   opts->check_symmetric = 0;
+  opts->shard_index = 0;
+  opts->shard_count = 1;
+  opts->profile = 0;
 }
 
 int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_engine** out) {
@@ -615,7 +680,7 @@ int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d_J, doub
   if (opts) o = *opts;
   if (o.fp32_cut != 0.0) return fail(LAI_ENOTSUP, "mixed precision not enabled in this build");
   LAI_CUDA_TRY(cudaSetDevice(engine->device));
-  return run_jk(engine, d_D, d_J, d_K, (cudaStream_t)stream, report, false);
+  return run_jk(engine, d_D, d_J, d_K, (cudaStream_t)stream, o, report, false);
 }
 
 int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double* J, double* K,
@@ -646,7 +711,7 @@ int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double* J, dou
   cudaStream_t s = engine->stream;
   LAI_CUDA_TRY(cudaMemcpyAsync(engine->d_D.p, D, bytes, cudaMemcpyHostToDevice, s));
   if (int rc = run_jk(engine, engine->d_D.as<double>(), engine->d_J.as<double>(),
-                      engine->d_K.as<double>(), s, report, true))
+                      engine->d_K.as<double>(), s, o, report, true))
     return rc;
   LAI_CUDA_TRY(cudaMemcpyAsync(J, engine->d_J.p, bytes, cudaMemcpyDeviceToHost, s));
   LAI_CUDA_TRY(cudaMemcpyAsync(K, engine->d_K.p, bytes, cudaMemcpyDeviceToHost, s));
@@ -717,6 +782,89 @@ int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_capacity,
     qo += bp.total;
     vo += bp.total * vals_per[b];
   }
+  return LAI_OK;
+}
+
+int lai_jk_last_profile(lai_engine* engine, int capacity, double* ms, double* alg_flops,
+                        int64_t* quartets, int* lclass) {
+  if (!engine) return fail(LAI_EINVAL, "lai_jk_last_profile: null engine");
+  const int n = engine->prof_n;
+  if (capacity < n || !ms) return n;
+  for (int i = 0; i < n; ++i) {
+    LAI_CUDA_TRY(cudaEventSynchronize(engine->prof_ev[2 * i + 1]));
+    float t = 0;
+    LAI_CUDA_TRY(cudaEventElapsedTime(&t, engine->prof_ev[2 * i], engine->prof_ev[2 * i + 1]));
+    ms[i] = t;
+    const auto& b = *engine->blocks[engine->prof_block[i]];
+    const auto& ca = *engine->classes[b.bra];
+    const auto& cb = *engine->classes[b.ket];
+    if (alg_flops) alg_flops[i] = b.alg_flops * (double)engine->prof_quartets[i];
+    if (quartets) quartets[i] = engine->prof_quartets[i];
+    if (lclass) {
+      lclass[4 * i] = ca.la; lclass[4 * i + 1] = ca.lb;
+      lclass[4 * i + 2] = cb.la; lclass[4 * i + 3] = cb.lb;
+    }
+  }
+  return n;
+}
+
+int64_t lai_engine_quartet_count(lai_engine* engine) {
+  if (!engine) return -1;
+  int64_t n = 0;
+  for (auto& b : engine->blocks) n += b->total;
+  return n;
+}
+
+int lai_engine_sample_quartets(lai_engine* engine, int64_t n, uint64_t seed, int32_t* quartets) {
+  if (!engine || n < 0 || (n > 0 && !quartets)) return fail(LAI_EINVAL, "lai_engine_sample_quartets");
+  std::vector<int64_t> pref(engine->blocks.size() + 1, 0);
+  for (size_t b = 0; b < engine->blocks.size(); ++b) pref[b + 1] = pref[b] + engine->blocks[b]->total;
+  const int64_t total = pref.back();
+  if (total == 0) return n == 0 ? LAI_OK : fail(LAI_ESTATE, "engine has no quartets");
+  uint64_t st = seed;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t t = (int64_t)(mix64(st) % (uint64_t)total);
+    const size_t b = std::upper_bound(pref.begin(), pref.end(), t) - pref.begin() - 1;
+    const auto& bp = *engine->blocks[b];
+    const int64_t tl = t - pref[b];
+    const int p = (int)(std::upper_bound(bp.offsets.begin(), bp.offsets.end(), tl) - bp.offsets.begin() - 1);
+    const int q = (int)(tl - bp.offsets[p]);
+    const auto& ca = *engine->classes[bp.bra];
+    const auto& cb = *engine->classes[bp.ket];
+    quartets[4 * i] = ca.sa[p];
+    quartets[4 * i + 1] = ca.sb[p];
+    quartets[4 * i + 2] = cb.sa[q];
+    quartets[4 * i + 3] = cb.sb[q];
+  }
+  return LAI_OK;
+}
+
+int lai_probe_fp64_peak(int device, double* tflops) {
+  if (!tflops) return fail(LAI_EINVAL, "lai_probe_fp64_peak: null output");
+  LAI_CUDA_TRY(cudaSetDevice(device));
+  int sms = 0;
+  LAI_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  DevBuf out;
+  LAI_CUDA_TRY(out.alloc(8));
+  cudaEvent_t a, b;
+  LAI_CUDA_TRY(cudaEventCreate(&a));
+  LAI_CUDA_TRY(cudaEventCreate(&b));
+  const int threads = 256, blocks = sms * 8, iters = 4096;
+  fp64_fma_probe<<<blocks, threads>>>(out.as<double>(), 64);  // warm-up
+  double best = 0;
+  for (int rep = 0; rep < 3; ++rep) {
+    LAI_CUDA_TRY(cudaEventRecord(a));
+    fp64_fma_probe<<<blocks, threads>>>(out.as<double>(), iters);
+    LAI_CUDA_TRY(cudaEventRecord(b));
+    LAI_CUDA_TRY(cudaEventSynchronize(b));
+    float ms = 0;
+    LAI_CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+    const double fl = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+    best = std::max(best, fl / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *tflops = best;
   return LAI_OK;
 }
 

@@ -132,11 +132,21 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
   const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
   const int W = g.LCD + 1;
 
-  for (int64_t t = gwarp; t < blk.total; t += nwarps) {
+  // each warp owns a contiguous run of quartets: one search, then p advances
+  const int64_t nq_all = blk.total - blk.t_begin;
+  const int64_t per = (nq_all + nwarps - 1) / nwarps;
+  const int64_t tbeg = blk.t_begin + gwarp * per;
+  const int64_t tend = min(blk.total, tbeg + per);
+  int p = -1;
+  for (int64_t t = tbeg; t < tend; ++t) {
+    const int64_t tl = t - blk.t_begin;
     // ---- locate the quartet ----
-    int p = 0;
-    if (lane == 0) p = find_bra(blk.offsets, nbra, t);
-    p = __shfl_sync(0xffffffffu, p, 0);
+    if (p < 0) {
+      if (lane == 0) p = find_bra(blk.offsets, nbra, t);
+      p = __shfl_sync(0xffffffffu, p, 0);
+    } else {
+      while (t >= __ldg(blk.offsets + p + 1)) ++p;
+    }
     const int q = (blk.qbegin ? __ldg(blk.qbegin + p) : 0) + (int)(t - __ldg(blk.offsets + p));
     const double AB[3] = {__ldg(blk.bra.AB + p), __ldg(blk.bra.AB + nbra + p),
                           __ldg(blk.bra.AB + 2 * nbra + p)};
@@ -298,7 +308,7 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
         v *= na_f * norm_factor(g.lb, b) * norm_factor(g.lc, c) * norm_factor(g.ld, d);
         O[i] = v;
         if (args.mode == MODE_RAW) {
-          args.raw_out[(size_t)t * g.na * g.nb * ncd + (size_t)a * g.nb * ncd + i] = v;
+          args.raw_out[(size_t)tl * g.na * g.nb * ncd + (size_t)a * g.nb * ncd + i] = v;
         } else if (args.mode == MODE_SCHWARZ) {
           if (c == a && d == b) smax = fmax(smax, fabs(v));
         }
@@ -364,7 +374,7 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
       }
     } else if (args.mode == MODE_RAW) {
       if (lane == 0) {
-        int* m = args.raw_meta + 4 * t;
+        int* m = args.raw_meta + 4 * tl;
         m[0] = fa; m[1] = fb; m[2] = fc; m[3] = fd;
       }
     } else if (args.mode == MODE_SCHWARZ) {
@@ -379,7 +389,7 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
 
 int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
                    cudaStream_t stream, double* gscratch, size_t gscratch_doubles, int num_sms) {
-  if (blk.total <= 0) return 0;
+  if (blk.total - blk.t_begin <= 0) return 0;
   const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
   int warps = 4;
   const size_t smem_max = 227 * 1024;
@@ -388,7 +398,7 @@ int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesV
   if (g.per_warp < 0) return -1;
   const size_t smem = (size_t)g.per_warp * 8 * warps;
   // enough warps to cover the SMs several times; grid-stride inside
-  int64_t want = (blk.total + warps - 1) / warps;
+  int64_t want = (blk.total - blk.t_begin + warps - 1) / warps;
   int64_t cap = (int64_t)num_sms * 16;
   int grid = (int)(want < cap ? want : cap);
   if (g.G_in_global) {

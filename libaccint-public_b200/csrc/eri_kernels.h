@@ -11,8 +11,13 @@ namespace lai {
 // the class (la,lb|lc,ld) has a specialised kernel and it was launched, 0 if the
 // class is not covered (use the generic kernel), <0 on a launch error.
 int launch_small(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
-                 cudaStream_t stream, bool fp32);
+                 cudaStream_t stream, bool fp32, int num_sms);
 bool small_class_supported(int la, int lb, int lc, int ld);
+
+// Bra-sliced kernels for the medium classes (eri_sliced.cu); same return codes.
+int launch_sliced(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
+                  cudaStream_t stream, bool fp32, int num_sms);
+bool sliced_class_supported(int la, int lb, int lc, int ld);
 
 // Warp-per-quartet generic kernel (eri_generic.cu), any class with l <= 4.
 int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,

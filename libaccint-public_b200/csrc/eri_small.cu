@@ -4,9 +4,15 @@
 // Fock blocks all live in registers.  The same algorithm as eri_generic.cu (see
 // eri_device.cuh), unrolled.
 //
-// A warp covers 32 consecutive canonical quartets of a block; consecutive
-// quartets usually share the bra pair, so bra primitive data are warp-uniform
-// loads and ket primitive data are coalesced (SoA by pair index).
+// Persistent launch (a few blocks per SM, grid-stride over chunks of 32
+// consecutive canonical quartets, one per lane).  Consecutive quartets usually
+// share the bra pair, so bra primitive data are warp-uniform loads, ket primitive
+// data are coalesced (SoA by pair index), and the bra-pair Coulomb block J_ij is
+// summed across the warp before its atomic update.  Each block stages the lookup
+// table its root count needs in shared memory once (Boys grid for one root, the
+// class's Rys table otherwise), with row strides padded so that lanes reading
+// different rows hit different banks -- from global memory those per-lane
+// gathers would touch up to 32 cache lines per load instruction.
 //
 // Templated on the compute type R: double for the FP64 path, float for the FP32
 // part of a mixed-precision build (roots, recurrences and contraction in FP32;
@@ -17,6 +23,7 @@
 
 #include "eri_device.cuh"
 #include "eri_kernels.h"
+#include "eri_tables_smem.cuh"
 
 namespace lai {
 
@@ -30,26 +37,24 @@ __device__ __forceinline__ void sfor(F&& f) {
   }
 }
 
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs args,
-                                                        RysTablesView tab) {
+__device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKArgs& args,
+                                              const RysTablesView& tab,
+                                              const double* __restrict__ stab, int64_t t, int p,
+                                              bool active, bool uniform_bra) {
   constexpr int LAB = LA + LB, LCD = LC + LD;
   constexpr int NR = (LAB + LCD) / 2 + 1;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr int NE = ncart_range(LA, LAB), NF = ncart_range(LC, LCD);
   constexpr int W = LCD + 1;
-
-  const int lane = threadIdx.x & 31;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t t0 = t - lane;
-  if (t0 >= blk.total) return;
   const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
-  int p = 0;
-  if (lane == 0) p = find_bra(blk.offsets, nbra, t0);
-  p = __shfl_sync(0xffffffffu, p, 0);
-  const bool active = t < blk.total;
-  if (!active) return;
-  while (t >= __ldg(blk.offsets + p + 1)) ++p;
   const int q = (blk.qbegin ? __ldg(blk.qbegin + p) : 0) + (int)(t - __ldg(blk.offsets + p));
 
   const int Kab = blk.bra.Ka * blk.bra.Kb;
@@ -85,7 +90,7 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
       const R T = zeta * rz * (PQx * PQx + PQy * PQy + PQz * PQz);
       const R pref = cab * ccd * rs;
       R u[NR], w[NR];
-      rys_roots_table<R>(NR, T, tab, u, w);
+      rys_smem<NR, R>(T, stab, tab, u, w);
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
         const R ur = u[r];
@@ -224,14 +229,17 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
   const int fa = __ldg(blk.bra.func_a + p), fb = __ldg(blk.bra.func_b + p);
   const int fc = __ldg(blk.ket.func_a + q), fd = __ldg(blk.ket.func_b + q);
   if (args.mode == MODE_RAW) {
-    double* o = args.raw_out + (size_t)t * (NA * NB * NC * ND);
+    if (!active) return;
+    const int64_t tl = t - blk.t_begin;
+    double* o = args.raw_out + (size_t)tl * (NA * NB * NC * ND);
 #pragma unroll
     for (int i = 0; i < NA * NB * NC * ND; ++i) o[i] = V[i];
-    int* m = args.raw_meta + 4 * t;
+    int* m = args.raw_meta + 4 * tl;
     m[0] = fa; m[1] = fb; m[2] = fc; m[3] = fd;
     return;
   }
   if (args.mode == MODE_SCHWARZ) {
+    if (!active) return;
     double mx = 0.0;
 #pragma unroll
     for (int a = 0; a < NA; ++a)
@@ -243,7 +251,7 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
   }
 
   // ---- 8-fold symmetric digestion: J' += 2 s g D, K' += s g D ----
-  const double sym = quartet_weight(blk, p, q);
+  const double sym = active ? quartet_weight(blk, p, q) : 0.0;
   const double* __restrict__ D = args.D;
   const int nbf = args.nbf;
   double* __restrict__ J = args.J;
@@ -259,7 +267,13 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
       double v = 0.0;
 #pragma unroll
       for (int cd = 0; cd < NC * ND; ++cd) v += V[ab * NC * ND + cd] * Dk[cd];
-      atomicAdd(J + (size_t)(fa + ab / NB) * nbf + fb + ab % NB, 2.0 * sym * v);
+      v *= 2.0 * sym;
+      if (uniform_bra) {  // every lane has the same bra pair: one atomic per warp
+        v = warp_sum(v);
+        if ((threadIdx.x & 31) == 0) atomicAdd(J + (size_t)(fa + ab / NB) * nbf + fb + ab % NB, v);
+      } else if (active) {
+        atomicAdd(J + (size_t)(fa + ab / NB) * nbf + fb + ab % NB, v);
+      }
     }
   }
   {  // J_kl[c][d] = sum_ab V D_ij
@@ -273,7 +287,7 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
       double v = 0.0;
 #pragma unroll
       for (int ab = 0; ab < NA * NB; ++ab) v += V[ab * NC * ND + cd] * Di[ab];
-      atomicAdd(J + (size_t)(fc + cd / ND) * nbf + fd + cd % ND, 2.0 * sym * v);
+      if (active) atomicAdd(J + (size_t)(fc + cd / ND) * nbf + fd + cd % ND, 2.0 * sym * v);
     }
   }
   {  // K_ik[a][c] = sum_bd V D_jl
@@ -291,7 +305,7 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
         for (int b = 0; b < NB; ++b)
 #pragma unroll
           for (int d = 0; d < ND; ++d) v += V[((a * NB + b) * NC + c) * ND + d] * Dx[b * ND + d];
-        atomicAdd(K + (size_t)(fa + a) * nbf + fc + c, sym * v);
+        if (active) atomicAdd(K + (size_t)(fa + a) * nbf + fc + c, sym * v);
       }
   }
   {  // K_il[a][d] = sum_bc V D_jk
@@ -309,7 +323,7 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
         for (int b = 0; b < NB; ++b)
 #pragma unroll
           for (int c = 0; c < NC; ++c) v += V[((a * NB + b) * NC + c) * ND + d] * Dx[b * NC + c];
-        atomicAdd(K + (size_t)(fa + a) * nbf + fd + d, sym * v);
+        if (active) atomicAdd(K + (size_t)(fa + a) * nbf + fd + d, sym * v);
       }
   }
   {  // K_jk[b][c] = sum_ad V D_il
@@ -327,7 +341,7 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
         for (int a = 0; a < NA; ++a)
 #pragma unroll
           for (int d = 0; d < ND; ++d) v += V[((a * NB + b) * NC + c) * ND + d] * Dx[a * ND + d];
-        atomicAdd(K + (size_t)(fb + b) * nbf + fc + c, sym * v);
+        if (active) atomicAdd(K + (size_t)(fb + b) * nbf + fc + c, sym * v);
       }
   }
   {  // K_jl[b][d] = sum_ac V D_ik
@@ -345,21 +359,63 @@ __global__ void __launch_bounds__(128) eri_small_kernel(QuartetBlock blk, JKArgs
         for (int a = 0; a < NA; ++a)
 #pragma unroll
           for (int c = 0; c < NC; ++c) v += V[((a * NB + b) * NC + c) * ND + d] * Dx[a * NC + c];
-        atomicAdd(K + (size_t)(fb + b) * nbf + fd + d, sym * v);
+        if (active) atomicAdd(K + (size_t)(fb + b) * nbf + fd + d, sym * v);
       }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(256) eri_small_kernel(QuartetBlock blk, JKArgs args,
+                                                        RysTablesView tab) {
+  constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+  extern __shared__ double stab[];
+  stage_table<NR>(stab, tab);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t nq = blk.total - blk.t_begin;
+  const int64_t nchunks = (nq + 31) >> 5;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int nbra = blk.bra.npairs;
+  for (int64_t c = wid; c < nchunks; c += nw) {
+    const int64_t t0 = blk.t_begin + (c << 5);
+    const int64_t t = t0 + lane;
+    const bool active = t < blk.total;
+    const int64_t te = active ? t : blk.total - 1;
+    int p = 0;
+    if (lane == 0) p = find_bra(blk.offsets, nbra, t0);
+    p = __shfl_sync(0xffffffffu, p, 0);
+    const int p0 = p;
+    while (te >= __ldg(blk.offsets + p + 1)) ++p;
+    const bool uniform = __all_sync(0xffffffffu, p == p0);
+    small_quartet<LA, LB, LC, LD, R>(blk, args, tab, stab, te, p, active, uniform);
   }
 }
 
 template <int LA, int LB, int LC, int LD>
 int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
-               cudaStream_t stream, bool fp32) {
-  const int threads = 128;
-  const int64_t blocks = (blk.total + threads - 1) / threads;
-  if (blocks > 0x7fffffffLL) return -2;
-  if (fp32)
-    eri_small_kernel<LA, LB, LC, LD, float><<<(unsigned)blocks, threads, 0, stream>>>(blk, args, tab);
-  else
-    eri_small_kernel<LA, LB, LC, LD, double><<<(unsigned)blocks, threads, 0, stream>>>(blk, args, tab);
+               cudaStream_t stream, bool fp32, int num_sms) {
+  constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+  const int threads = 256;
+  const size_t smem = sizeof(double) * table_doubles<NR>();
+  const int64_t nchunks = (blk.total - blk.t_begin + 31) / 32;
+  if (nchunks <= 0) return 1;
+  auto kern = fp32 ? eri_small_kernel<LA, LB, LC, LD, float> : eri_small_kernel<LA, LB, LC, LD, double>;
+  static bool attr[2] = {false, false};
+  int per_sm = 0;
+  static int per_sm_cache[2] = {0, 0};
+  if (!attr[fp32]) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return -3;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cache[fp32], kern, threads, smem) != cudaSuccess)
+      return -3;
+    attr[fp32] = true;
+  }
+  per_sm = per_sm_cache[fp32] > 0 ? per_sm_cache[fp32] : 1;
+  const int64_t want = (nchunks + (threads / 32) - 1) / (threads / 32);
+  const int64_t cap = (int64_t)num_sms * per_sm;
+  const int grid = (int)(want < cap ? want : cap);
+  kern<<<grid, threads, smem, stream>>>(blk, args, tab);
   return cudaGetLastError() == cudaSuccess ? 1 : -3;
 }
 
@@ -368,7 +424,7 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
 #define LAI_SMALL_CLASSES(X) \
   X(0, 0, 0, 0) X(1, 0, 0, 0) X(1, 0, 1, 0) X(1, 1, 0, 0) X(1, 1, 1, 0) X(2, 0, 0, 0) \
   X(2, 0, 1, 0) X(2, 0, 2, 0) X(2, 1, 0, 0) X(2, 2, 0, 0) X(3, 0, 0, 0) X(3, 0, 1, 0)   \
-  X(3, 1, 0, 0) X(4, 0, 0, 0)
+  X(3, 1, 0, 0) X(4, 0, 0, 0) X(1, 1, 1, 1) X(2, 0, 1, 1) X(2, 1, 1, 0) X(2, 1, 2, 0) X(2, 2, 1, 0)
 
 bool small_class_supported(int la, int lb, int lc, int ld) {
 #define X(a, b, c, d) if (la == a && lb == b && lc == c && ld == d) return true;
@@ -378,10 +434,10 @@ bool small_class_supported(int la, int lb, int lc, int ld) {
 }
 
 int launch_small(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
-                 cudaStream_t stream, bool fp32) {
+                 cudaStream_t stream, bool fp32, int num_sms) {
   const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
 #define X(a, b, c, d) \
-  if (la == a && lb == b && lc == c && ld == d) return launch_one<a, b, c, d>(blk, args, tab, stream, fp32);
+  if (la == a && lb == b && lc == c && ld == d) return launch_one<a, b, c, d>(blk, args, tab, stream, fp32, num_sms);
   LAI_SMALL_CLASSES(X)
 #undef X
   return 0;

@@ -61,6 +61,7 @@ struct QuartetBlock {
   PairClassDev bra, ket;
   const int64_t* offsets;   // [bra.npairs + 1]
   const int* qbegin;        // [bra.npairs] or nullptr
+  int64_t t_begin;          // a launch covers flat quartet indices [t_begin, total)
   int64_t total;
   int same_class;
 };

@@ -105,35 +105,66 @@ class Engine:
         _lib.check(_lib.lib().lai_engine_schwarz(self._h, Q.ctypes.data))
         return Q
 
-    def jk(self, D, fp32_cut=0.0, check_symmetric=False):
-        """(J, K, report) for a host density D."""
+    @staticmethod
+    def _opts(fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False):
+        opts = _lib.JKOpts()
+        _lib.lib().lai_jk_opts_default(ctypes.byref(opts))
+        opts.fp32_cut = fp32_cut
+        opts.check_symmetric = int(check_symmetric)
+        opts.shard_index, opts.shard_count = shard
+        opts.profile = int(profile)
+        return opts
+
+    def jk(self, D, fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False, out=None):
+        """(J, K, report) for a host density D.  ``out`` = (J, K) host arrays to
+        fill (e.g. pinned memory); ``shard`` = (index, count) computes one
+        rank's partial J/K of a multi-GPU build."""
         L = _lib.lib()
         n = self.basis.nbf
         D = np.ascontiguousarray(D, dtype=np.float64)
         if D.shape != (n, n):
             raise ValueError(f"density must be {n}x{n}")
-        J = np.empty((n, n))
-        K = np.empty((n, n))
-        opts = _lib.JKOpts()
-        L.lai_jk_opts_default(ctypes.byref(opts))
-        opts.fp32_cut = fp32_cut
-        opts.check_symmetric = int(check_symmetric)
+        if out is None:
+            J = np.empty((n, n))
+            K = np.empty((n, n))
+        else:
+            J, K = out
+        opts = self._opts(fp32_cut, check_symmetric, shard, profile)
         rep = _lib.JKReport()
         _lib.check(L.lai_jk_build(self._h, D.ctypes.data, n, J.ctypes.data, K.ctypes.data,
                                   ctypes.byref(opts), ctypes.byref(rep)))
         return J, K, rep
 
-    def jk_device(self, d_D, d_J, d_K, stream=0, fp32_cut=0.0):
+    def jk_device(self, d_D, d_J, d_K, stream=0, fp32_cut=0.0, shard=(0, 1), profile=False):
         """Device-pointer variant (integers from torch.Tensor.data_ptr())."""
         L = _lib.lib()
-        opts = _lib.JKOpts()
-        L.lai_jk_opts_default(ctypes.byref(opts))
-        opts.fp32_cut = fp32_cut
+        opts = self._opts(fp32_cut, False, shard, profile)
         rep = _lib.JKReport()
         _lib.check(L.lai_jk_build_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
                                          ctypes.c_void_p(d_K), ctypes.c_void_p(stream),
                                          ctypes.byref(opts), ctypes.byref(rep)))
         return rep
+
+    def last_profile(self):
+        """Per-launch (ms, alg_flops, quartets, (la,lb,lc,ld)) of the last profiled build."""
+        L = _lib.lib()
+        n = L.lai_jk_last_profile(self._h, 0, None, None, None, None)
+        ms = np.zeros(n)
+        fl = np.zeros(n)
+        nq = np.zeros(n, dtype=np.int64)
+        lc = np.zeros(4 * n, dtype=np.int32)
+        got = L.lai_jk_last_profile(self._h, n, ms.ctypes.data, fl.ctypes.data, nq.ctypes.data, lc.ctypes.data)
+        if got < 0:
+            _lib.check(got)
+        return ms, fl, nq, lc.reshape(-1, 4)
+
+    def quartet_count(self):
+        return int(_lib.lib().lai_engine_quartet_count(self._h))
+
+    def sample_quartets(self, n, seed=0):
+        q = np.zeros((n, 4), dtype=np.int32)
+        _lib.check(_lib.lib().lai_engine_sample_quartets(self._h, n, seed, q.ctypes.data))
+        return q
 
     def compute_batch_screened(self, op=None):
         """All canonical screened quartets: (values, meta) with meta rows
@@ -178,6 +209,13 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def probe_fp64_peak(device=0):
+    """FP64 FMA throughput of the device (TFLOP/s) from a register-resident FMA loop."""
+    v = ctypes.c_double()
+    _lib.check(_lib.lib().lai_probe_fp64_peak(device, ctypes.byref(v)))
+    return v.value
 
 
 def jk(basis, D, threshold=1e-12, fp32_cut=0.0):

@@ -73,6 +73,7 @@ def reference():
         L.ref_jk_screened_sym.argtypes = [_P, _P, _P, _P, _D]
         L.ref_eri_quartet.argtypes = [_P, _L, _L, _L, _L, _P]
         L.ref_schwarz.argtypes = [_P, _P]
+        L.ref_schwarz_parallel.argtypes = [_P, _P, _I]
         L.ref_rys.argtypes = [_I, _D, _P, _P]
         L.ref_boys.argtypes = [_I, _D, _P]
         L.ref_time_quartets.restype = _D
@@ -208,6 +209,13 @@ class RefBasis:
         self.R.ref_schwarz(self.h, Q.ctypes.data)
         return Q
 
+    def schwarz_parallel(self, nthreads=0):
+        Q = np.zeros((self.nshell, self.nshell))
+        rc = self.R.ref_schwarz_parallel(self.h, Q.ctypes.data, nthreads)
+        if rc != 0:
+            raise RuntimeError(self.R.ref_last_error().decode())
+        return Q
+
     def time_quartets(self, D, quartets, nthreads=0, want_jk=False):
         n = self.nbf
         D = np.ascontiguousarray(D, dtype=np.float64)
@@ -238,3 +246,34 @@ class RefBasis:
         if getattr(self, "h", None):
             self.R.ref_basis_free(self.h)
             self.h = None
+
+
+class CanonicalQuartets:
+    """The canonical Schwarz-screened shell quartets of a basis, from a Schwarz
+    matrix Q: unordered pairs {P, Q'} of shell pairs with Q_P * Q_Q' >= thr
+    (the reference's canonical loop, include/libaccint/engine/engine.hpp:1815-1858,
+    with passes_screening).  Counts them and draws uniform samples, without
+    materializing the list."""
+
+    def __init__(self, Q, thr):
+        n = Q.shape[0]
+        i, j = np.triu_indices(n)
+        q = Q[i, j]
+        order = np.argsort(-q, kind="stable")
+        self.pi, self.pj, self.q = i[order], j[order], q[order]
+        # partners of sorted pair p: sorted positions r <= p with q[r] * q[p] >= thr
+        neg = -self.q
+        with np.errstate(divide="ignore"):
+            lim = np.where(self.q > 0, thr / np.where(self.q > 0, self.q, 1.0), np.inf)
+        cut = np.searchsorted(neg, -lim, side="right")
+        # exact test at the boundary (product form, as the reference compares)
+        self.count = np.minimum(cut, np.arange(len(self.q)) + 1).astype(np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.count)])
+        self.total = int(self.offsets[-1])
+
+    def sample(self, n, seed=0):
+        rng = np.random.default_rng(seed)
+        t = rng.integers(0, self.total, size=n)
+        p = np.searchsorted(self.offsets, t, side="right") - 1
+        r = t - self.offsets[p]
+        return np.stack([self.pi[p], self.pj[p], self.pi[r], self.pj[r]], axis=1).astype(np.int64)

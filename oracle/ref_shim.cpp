@@ -29,7 +29,9 @@
 
 #include <omp.h>
 
+#include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -194,6 +196,38 @@ int ref_schwarz(void* h, double* Q) {
         const Size n = basis.n_shells();
         for (Size i = 0; i < n; ++i)
             for (Size j = i; j < n; ++j) Q[i * n + j] = Q[j * n + i] = sb(i, j);
+        return 0;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1;
+    }
+}
+
+// Same bounds as SchwarzBounds(basis) (schwarz_bounds.cpp:20-59: Q_ij =
+// sqrt(max_ab |(ab|ab)|) from kernels::compute_eri), with the pair loop spread
+// over OpenMP threads.  Q is the full nshell x nshell matrix.
+int ref_schwarz_parallel(void* h, double* Q, int nthreads) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(h)->basis;
+        const long n = (long)basis.n_shells();
+        if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+        {
+            TwoElectronBuffer<0> buf;
+#pragma omp for schedule(dynamic, 16)
+            for (long ij = 0; ij < n * n; ++ij) {
+                const long i = ij / n, j = ij % n;
+                if (j < i) continue;
+                const auto& si = basis.shell(i);
+                const auto& sj = basis.shell(j);
+                kernels::compute_eri(si, sj, si, sj, buf);
+                double mx = 0.0;
+                for (int a = 0; a < si.n_functions(); ++a)
+                    for (int b = 0; b < sj.n_functions(); ++b)
+                        mx = std::max(mx, std::abs(buf(a, b, a, b)));
+                Q[i * n + j] = Q[j * n + i] = std::sqrt(mx);
+            }
+        }
         return 0;
     } catch (const std::exception& ex) {
         set_err(ex.what());
