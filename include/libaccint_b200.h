@@ -86,6 +86,10 @@ LAI_API int lai_basis_shell(const lai_basis* basis, int s, int* l, int* nprim, d
 typedef struct {
   double schwarz_threshold; /* pass iff Q_ij*Q_kl >= threshold (default 1e-12) */
   int device;               /* CUDA device ordinal (default 0)                  */
+  double prim_threshold;    /* skip primitive quartets whose primitive Schwarz
+                               bound q_ab*q_cd is below this (no counterpart in
+                               the reference); < 0 = 1e-3 * schwarz_threshold
+                               (default), 0 = keep every primitive quartet       */
 } lai_engine_opts;
 LAI_API void lai_engine_opts_default(lai_engine_opts* opts);
 LAI_API int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_engine** out);
@@ -157,10 +161,14 @@ LAI_API int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_c
  * profiling of this path).
  * ------------------------------------------------------------------------- */
 /* Per-launch device times of the last build made with opts.profile = 1.  For
- * launch i: ms[i], algorithmic FLOP alg_flops[i], quartets[i], class
- * (la,lb,lc,ld) in lclass[4*i..4*i+3].  Returns the launch count, or < 0. */
+ * launch i: ms[i]; algorithmic FLOP with every nonzero primitive quartet counted
+ * (alg_flops) and with only the primitive quartets that passed the primitive
+ * cut and were executed (alg_flops_executed); quartets[i]; primitive quartets
+ * executed (prim_quartets[i]); class (la,lb,lc,ld) in lclass[4*i..4*i+3].
+ * Any output may be NULL except ms.  Returns the launch count, or < 0. */
 LAI_API int lai_jk_last_profile(lai_engine* engine, int capacity, double* ms, double* alg_flops,
-                                int64_t* quartets, int* lclass);
+                                double* alg_flops_executed, int64_t* quartets,
+                                int64_t* prim_quartets, int* lclass);
 /* n canonical screened quartets drawn uniformly (seeded) from all of the
  * engine's quartets, as shell indices [n][4] in the order the engine computes
  * them.  Used to time the reference CPU path on a bounded sample. */

@@ -31,7 +31,8 @@ class LibAccIntError(RuntimeError):
 
 
 class EngineOpts(ctypes.Structure):
-    _fields_ = [("schwarz_threshold", ctypes.c_double), ("device", ctypes.c_int)]
+    _fields_ = [("schwarz_threshold", ctypes.c_double), ("device", ctypes.c_int),
+                ("prim_threshold", ctypes.c_double)]
 
 
 class JKOpts(ctypes.Structure):
@@ -80,7 +81,7 @@ def lib():
         "lai_jk_build_device": (I, [P, P, P, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKReport)]),
         "lai_eri_batch_screened": (I, [P, P, ctypes.c_size_t, P, ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
-        "lai_jk_last_profile": (I, [P, I, P, P, P, P]),
+        "lai_jk_last_profile": (I, [P, I, P, P, P, P, P, P]),
         "lai_engine_sample_quartets": (I, [P, ctypes.c_int64, ctypes.c_uint64, P]),
         "lai_engine_quartet_count": (ctypes.c_int64, [P]),
         "lai_probe_fp64_peak": (I, [I, ctypes.POINTER(ctypes.c_double)]),

@@ -193,6 +193,7 @@ namespace {
 
 struct PairClassHost {
   int la, lb, Ka, Kb;
+  double qprim_max = 0.0;
   std::vector<int> sa, sb, fa, fb;  // shell and function indices (oriented)
   std::vector<double> Q;
   std::vector<double> AB;          // SoA [3][n]
@@ -206,6 +207,7 @@ struct PairClassHost {
     v.shell_a = d_sa.as<int>(); v.shell_b = d_sb.as<int>();
     v.func_a = d_fa.as<int>(); v.func_b = d_fb.as<int>();
     v.Q = d_Q.as<double>(); v.AB = d_AB.as<double>(); v.prim = d_prim.as<double>();
+    v.qprim_max = qprim_max;
     return v;
   }
 };
@@ -215,21 +217,29 @@ struct ClassPairBlock {
   std::vector<int64_t> offsets; // host copy
   DevBuf d_offsets;
   int64_t total = 0;
-  double alg_flops = 0;         // per quartet of this block
+  double alg_flops = 0;         // per quartet of this block (all nonzero primitives)
+  double flops_per_prim = 0;    // per primitive quartet
+  double flops_per_quartet = 0; // per contracted quartet (normalization + digestion)
 };
 
 // Algorithmic FP work of one canonical quartet (one unit), the single accounting
 // used for roofline fractions:  P (40 + 64 n + n (20 + T2D + 4 Ncart)) + 25 Ncart
 // with P the product of nonzero primitive counts, n the root count and
 // T2D = 3 [5 (La+Lb+1)(Lc+Ld+1) + 2 Lb (La+Lb+1)(Lc+Ld+1)(Ld+1) + 2 Ld (La+1)(Lb+1)(Lc+Ld+1)].
-double alg_work(int la, int lb, int lc, int ld, int Ka, int Kb, int Kc, int Kd) {
-  const double P = (double)Ka * Kb * Kc * Kd;
+double alg_per_prim(int la, int lb, int lc, int ld) {
   const int n = (la + lb + lc + ld) / 2 + 1;
   const double nc = (double)lai::ncart(la) * lai::ncart(lb) * lai::ncart(lc) * lai::ncart(ld);
   const double t2d = 3.0 * (5.0 * (la + lb + 1) * (lc + ld + 1) +
                             2.0 * lb * (la + lb + 1) * (lc + ld + 1) * (ld + 1) +
                             2.0 * ld * (la + 1) * (lb + 1) * (lc + ld + 1));
-  return P * (40.0 + 64.0 * n + n * (20.0 + t2d + 4.0 * nc)) + 25.0 * nc;
+  return 40.0 + 64.0 * n + n * (20.0 + t2d + 4.0 * nc);
+}
+double alg_per_quartet(int la, int lb, int lc, int ld) {
+  return 25.0 * lai::ncart(la) * lai::ncart(lb) * lai::ncart(lc) * lai::ncart(ld);
+}
+double alg_work(int la, int lb, int lc, int ld, int Ka, int Kb, int Kc, int Kd) {
+  const double P = (double)Ka * Kb * Kc * Kd;
+  return P * alg_per_prim(la, lb, lc, ld) + alg_per_quartet(la, lb, lc, ld);
 }
 
 __global__ void symmetrize_kernel(const double* __restrict__ Jp, const double* __restrict__ Kp,
@@ -249,6 +259,7 @@ struct lai_engine {
   int device = 0;
   int num_sms = 148;
   double thr = 1e-12;
+  double prim_eps = 1e-15;
   cudaStream_t stream = nullptr;
   DevBuf d_coef, d_hx2, d_hw, d_boys;
   lai::RysTablesView tab{};
@@ -264,6 +275,7 @@ struct lai_engine {
   std::vector<cudaEvent_t> prof_ev;
   std::vector<int> prof_block;
   std::vector<int64_t> prof_quartets;
+  DevBuf d_prof_prims;
   int prof_n = 0;
   ~lai_engine() {
     for (auto e : prof_ev) cudaEventDestroy(e);
@@ -422,6 +434,60 @@ int compute_schwarz(lai_engine* E) {
   return LAI_OK;
 }
 
+// Primitive Schwarz bounds: every primitive pair of every shell pair is run as a
+// one-primitive pair through the diagonal kernel, q = sqrt(max |(a_p b_q|a_p b_q)|)
+// (contraction coefficients included).  By the Schwarz inequality a primitive
+// quartet contributes at most q_ab q_cd to any integral of its quartet.
+int compute_prim_schwarz(lai_engine* E) {
+  for (auto& cp : E->classes) {
+    auto& c = *cp;
+    const int n = c.n();
+    const int Kab = c.Ka * c.Kb;
+    const int ne = n * Kab;
+    if (ne == 0) continue;
+    PairClassHost pc;
+    pc.la = c.la; pc.lb = c.lb; pc.Ka = 1; pc.Kb = 1;
+    pc.sa.resize(ne); pc.sb.resize(ne); pc.fa.resize(ne); pc.fb.resize(ne);
+    pc.AB.resize(3 * (size_t)ne);
+    pc.prim.assign((size_t)lai::PF_COUNT * ne, 0.0);
+    for (int p = 0; p < n; ++p)
+      for (int t = 0; t < Kab; ++t) {
+        const int e = p * Kab + t;
+        pc.sa[e] = c.sa[p]; pc.sb[e] = c.sb[p]; pc.fa[e] = c.fa[p]; pc.fb[e] = c.fb[p];
+        for (int x = 0; x < 3; ++x) pc.AB[(size_t)x * ne + e] = c.AB[(size_t)x * n + p];
+        for (int f = 0; f < lai::PF_COUNT; ++f)
+          pc.prim[(size_t)f * ne + e] = c.prim[((size_t)f * Kab + t) * n + p];
+      }
+    if (int rc = upload_class(pc)) return rc;
+    std::vector<int64_t> off(ne + 1);
+    std::vector<int> qb(ne);
+    for (int e = 0; e <= ne; ++e) off[e] = e;
+    for (int e = 0; e < ne; ++e) qb[e] = e;
+    DevBuf d_off, d_qb, d_out;
+    LAI_CUDA_TRY(upload(d_off, off));
+    LAI_CUDA_TRY(upload(d_qb, qb));
+    LAI_CUDA_TRY(d_out.alloc(sizeof(double) * ne));
+    lai::QuartetBlock blk{};
+    blk.bra = blk.ket = pc.view();
+    blk.offsets = d_off.as<int64_t>();
+    blk.qbegin = d_qb.as<int>();
+    blk.total = ne;
+    blk.same_class = 1;
+    lai::JKArgs args{};
+    args.mode = lai::MODE_SCHWARZ;
+    args.schwarz_out = d_out.as<double>();
+    if (int rc = launch_block(E, blk, args)) return rc;
+    std::vector<double> q(ne);
+    LAI_CUDA_TRY(cudaMemcpyAsync(q.data(), d_out.p, sizeof(double) * ne, cudaMemcpyDeviceToHost,
+                                 E->stream));
+    LAI_CUDA_TRY(cudaStreamSynchronize(E->stream));
+    for (int p = 0; p < n; ++p)
+      for (int t = 0; t < Kab; ++t)
+        c.prim[((size_t)lai::PF_Q * Kab + t) * n + p] = q[(size_t)p * Kab + t];
+  }
+  return LAI_OK;
+}
+
 int sort_and_screen(lai_engine* E) {
   const int ns = (int)E->basis->shells.size();
   E->Q_all.assign((size_t)ns * ns, 0.0);
@@ -453,6 +519,20 @@ int sort_and_screen(lai_engine* E) {
       for (int f = 0; f < lai::PF_COUNT * Kab; ++f)
         prim[(size_t)f * keep + i] = c.prim[(size_t)f * n + idx[i]];
     }
+    // primitive pairs of each shell pair in descending primitive-Schwarz order
+    c.qprim_max = 0.0;
+    std::vector<int> tix(Kab);
+    std::vector<double> tmp(Kab);
+    for (int i = 0; i < keep; ++i) {
+      auto qat = [&](int t) { return prim[((size_t)lai::PF_Q * Kab + t) * keep + i]; };
+      std::iota(tix.begin(), tix.end(), 0);
+      std::stable_sort(tix.begin(), tix.end(), [&](int x, int y) { return qat(x) > qat(y); });
+      for (int f = 0; f < lai::PF_COUNT; ++f) {
+        for (int t = 0; t < Kab; ++t) tmp[t] = prim[((size_t)f * Kab + tix[t]) * keep + i];
+        for (int t = 0; t < Kab; ++t) prim[((size_t)f * Kab + t) * keep + i] = tmp[t];
+      }
+      c.qprim_max = std::max(c.qprim_max, qat(0));
+    }
     c.sa = perm(c.sa); c.sb = perm(c.sb); c.fa = perm(c.fa); c.fb = perm(c.fb);
     c.Q = std::move(Q); c.AB = std::move(AB); c.prim = std::move(prim);
     if (int rc = upload_class(c)) return rc;
@@ -483,6 +563,8 @@ int sort_and_screen(lai_engine* E) {
       blk->total = blk->offsets[ca.n()];
       if (blk->total == 0) continue;
       blk->alg_flops = alg_work(ca.la, ca.lb, cb.la, cb.lb, ca.Ka, ca.Kb, cb.Ka, cb.Kb);
+      blk->flops_per_prim = alg_per_prim(ca.la, ca.lb, cb.la, cb.lb);
+      blk->flops_per_quartet = alg_per_quartet(ca.la, ca.lb, cb.la, cb.lb);
       LAI_CUDA_TRY(upload(blk->d_offsets, blk->offsets));
       E->blocks.push_back(std::move(blk));
     }
@@ -521,6 +603,7 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
   args.K = E->d_Kp.as<double>();
   args.nbf = nbf;
   args.mode = lai::MODE_JK;
+  args.prim_eps = E->prim_eps;
   int launches = 0;
   int64_t nq = 0;
   double flops = 0;
@@ -533,6 +616,9 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
     }
     E->prof_block.clear();
     E->prof_quartets.clear();
+    if (E->d_prof_prims.bytes < sizeof(unsigned long long) * E->blocks.size())
+      LAI_CUDA_TRY(E->d_prof_prims.alloc(sizeof(unsigned long long) * std::max<size_t>(1, E->blocks.size())));
+    LAI_CUDA_TRY(cudaMemsetAsync(E->d_prof_prims.p, 0, E->d_prof_prims.bytes, stream));
   }
   E->prof_n = 0;
   for (size_t b = 0; b < E->blocks.size(); ++b) {
@@ -544,6 +630,7 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
     if (hi <= lo) continue;
     q.t_begin = lo;
     q.total = hi;
+    args.prim_count = o.profile ? E->d_prof_prims.as<unsigned long long>() + E->prof_n : nullptr;
     if (o.profile) LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n], stream));
     if (int rc = launch_block(E, q, args)) { E->stream = saved; return rc; }
     if (o.profile) {
@@ -606,6 +693,7 @@ void lai_engine_opts_default(lai_engine_opts* opts) {
   if (!opts) return;
   opts->schwarz_threshold = 1e-12;
   opts->device = 0;
+  opts->prim_threshold = -1.0;
 }
 
 void lai_jk_opts_default(lai_jk_opts* opts) {
@@ -632,6 +720,7 @@ int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_e
   E->basis = basis;
   E->device = o.device;
   E->thr = o.schwarz_threshold;
+  E->prim_eps = o.prim_threshold < 0.0 ? 1e-3 * o.schwarz_threshold : o.prim_threshold;
   LAI_CUDA_TRY(cudaDeviceGetAttribute(&E->num_sms, cudaDevAttrMultiProcessorCount, o.device));
   LAI_CUDA_TRY(cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking));
   LAI_CUDA_TRY(cudaEventCreate(&E->ev0));
@@ -654,6 +743,7 @@ int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_e
     if (int rc = upload_class(*c)) return rc;
   }
   if (int rc = compute_schwarz(E.get())) return rc;
+  if (int rc = compute_prim_schwarz(E.get())) return rc;
   if (int rc = sort_and_screen(E.get())) return rc;
   *out = E.release();
   return LAI_OK;
@@ -786,20 +876,30 @@ int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_capacity,
 }
 
 int lai_jk_last_profile(lai_engine* engine, int capacity, double* ms, double* alg_flops,
-                        int64_t* quartets, int* lclass) {
+                        double* alg_flops_executed, int64_t* quartets, int64_t* prim_quartets,
+                        int* lclass) {
   if (!engine) return fail(LAI_EINVAL, "lai_jk_last_profile: null engine");
   const int n = engine->prof_n;
   if (capacity < n || !ms) return n;
+  std::vector<unsigned long long> prims(n, 0);
+  if (n > 0) {
+    LAI_CUDA_TRY(cudaEventSynchronize(engine->prof_ev[2 * n - 1]));
+    LAI_CUDA_TRY(cudaMemcpy(prims.data(), engine->d_prof_prims.p, sizeof(unsigned long long) * n,
+                            cudaMemcpyDeviceToHost));
+  }
   for (int i = 0; i < n; ++i) {
-    LAI_CUDA_TRY(cudaEventSynchronize(engine->prof_ev[2 * i + 1]));
     float t = 0;
     LAI_CUDA_TRY(cudaEventElapsedTime(&t, engine->prof_ev[2 * i], engine->prof_ev[2 * i + 1]));
     ms[i] = t;
     const auto& b = *engine->blocks[engine->prof_block[i]];
     const auto& ca = *engine->classes[b.bra];
     const auto& cb = *engine->classes[b.ket];
-    if (alg_flops) alg_flops[i] = b.alg_flops * (double)engine->prof_quartets[i];
+    const double nq = (double)engine->prof_quartets[i];
+    if (alg_flops) alg_flops[i] = b.alg_flops * nq;
+    if (alg_flops_executed)
+      alg_flops_executed[i] = b.flops_per_prim * (double)prims[i] + b.flops_per_quartet * nq;
     if (quartets) quartets[i] = engine->prof_quartets[i];
+    if (prim_quartets) prim_quartets[i] = (int64_t)prims[i];
     if (lclass) {
       lclass[4 * i] = ca.la; lclass[4 * i + 1] = ca.lb;
       lclass[4 * i + 2] = cb.la; lclass[4 * i + 3] = cb.lb;

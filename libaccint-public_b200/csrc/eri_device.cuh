@@ -93,7 +93,17 @@ struct JKArgs {
   int* raw_meta;         // MODE_RAW: [quartet][4] first function index of a, b, c, d
   double* schwarz_out;   // MODE_SCHWARZ: [bra pair] sqrt(max |(ab|ab)|)
   unsigned int* status;  // device status word (0 = ok)
+  double prim_eps;       // skip primitive quartets with q_ab * q_cd < prim_eps (0 = none)
+  unsigned long long* prim_count;  // optional: += primitive quartets executed by the launch
 };
+
+// Add a per-lane count to a launch counter (one atomic per warp).
+__device__ __forceinline__ void count_prims(unsigned long long* ctr, unsigned int n) {
+  if (!ctr) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(ctr, (unsigned long long)n);
+}
 enum { MODE_JK = 0, MODE_RAW = 1, MODE_SCHWARZ = 2 };
 
 // Locate the bra pair p of flat quartet index t: largest p with offsets[p] <= t.

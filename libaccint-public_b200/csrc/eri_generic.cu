@@ -1,22 +1,26 @@
-// Generic warp-per-quartet Rys ERI kernel (any la..ld <= 4, runtime angular
-// momenta), fused with J/K digestion.  It is the path for the larger classes,
-// whose per-quartet state does not fit one thread's registers; the small classes
-// run in the thread-per-quartet kernels of eri_small.cu.
+// Generic warp-per-quartet Rys ERI kernel (any la..ld <= 4, run-time angular
+// momenta), fused with J/K digestion -- the path for the large classes that the
+// register-resident (eri_small.cu) and bra-sliced (eri_sliced.cu) kernels do not
+// cover.
 //
-// One warp owns one canonical quartet at a time (grid-stride over the block's
-// flat quartet range):
-//   * lanes split the (primitive quartet x root) items: each lane evaluates one
-//     root and builds that root's three 2D tables into shared memory;
-//   * lanes then split the (e0|f0) accumulator G: each lane owns up to kRmax
-//     entries in registers and sums Ix*Iy*Iz over the staged items;
-//   * G goes to shared memory; for each Cartesian component a of the bra's first
-//     shell the warp does the bra then ket transfer into an output tile
-//     O[b][c][d] and digests it: J_ij[a][:], K_ik[a][:], K_il[a][:] are complete
-//     per tile, J_kl, K_jk, K_jl accumulate in shared memory across tiles.
-// The reference's counterparts are eri_kernel<La,Lb,Lc,Ld> (thread per quartet,
-// src/device/cuda/kernels/eri_kernel.cu:227-461) followed by a separate
-// fock_accumulate_batch_kernel (src/device/cuda/consumers/fock_builder_gpu.cu:116-180)
-// that re-reads every integral from HBM; here no integral is written to HBM.
+// Per block, class-constant tables are built once in shared memory: the
+// Cartesian components of the (e0| and |f0) lists, and for the closed-form
+// transfer the row of (e0| needed by every (a, b, k) term with its binomial
+// weight and the exponents of (A-B).  Each warp then owns one canonical quartet
+// at a time (a contiguous run of quartets per warp):
+//   1. items = (primitive quartet x root); lanes build one item's three 2D tables
+//      each into shared memory (batches of up to 32 items);
+//   2. lanes sweep the (e0|f0) block G in tiles of 32 x kR entries held in
+//      registers, summing Ix*Iy*Iz over the staged items (G kept in shared memory
+//      or, for the largest classes, a per-warp slab of global scratch);
+//   3. per Cartesian component a of the bra's first shell: bra transfer into
+//      tmp[b][f], ket transfer + normalization into O[b][c][d], digestion:
+//      J_ij[a][:], K_ik[a][:], K_il[a][:] per tile, J_kl, K_jk, K_jl accumulated
+//      in shared memory over the tiles.
+// The reference counterpart is eri_kernel<La,Lb,Lc,Ld> (thread per quartet,
+// src/device/cuda/kernels/eri_kernel.cu:227-461) followed by the separate
+// fock_accumulate_batch_kernel (src/device/cuda/consumers/fock_builder_gpu.cu:116-180);
+// here no integral is written to HBM.
 #include <cuda_runtime.h>
 
 #include "eri_device.cuh"
@@ -26,19 +30,25 @@ namespace lai {
 
 namespace {
 
-constexpr int kRmax = 32;  // G entries per lane per pass
+constexpr int kR = 8;          // G entries per lane per tile
+constexpr int kMaxTerms = 12;  // max prod_x (b_x + 1) over components b with |b| <= 4
 
 struct GenericGeom {
   int la, lb, lc, ld;
-  int LAB, LCD;            // la+lb, lc+ld
+  int LAB, LCD;
   int na, nb, nc, nd;
-  int NE, NF, NEF;         // (e0| and |f0) component counts
-  int n;                   // roots
-  int nbt;                 // items staged per batch
-  int tsz;                 // (LAB+1)*(LCD+1)
-  // per-warp shared-memory layout (in doubles)
-  int off_tab, off_G, off_tmp, off_O, off_D, off_acc, per_warp;
+  int NE, NF, NEF;
+  int n;          // roots
+  int nbt;        // items staged per batch
+  int tsz;        // (LAB+1)*(LCD+1)
+  // class tables (shared by the block), ints
+  int off_ecomp, off_fcomp, off_brow, off_bexp, off_krow, off_kexp, class_ints;
+  // per-warp region (doubles)
+  int off_tab, off_G, off_tmp, off_O, off_D, off_acc, off_bcoef, off_kcoef, per_warp;
   int G_in_global;
+  __host__ __device__ size_t smem_bytes(int warps) const {
+    return (size_t)class_ints * 4 + (size_t)per_warp * 8 * warps;
+  }
 };
 
 __host__ GenericGeom make_geom(int la, int lb, int lc, int ld, size_t smem_limit, int warps) {
@@ -51,23 +61,31 @@ __host__ GenericGeom make_geom(int la, int lb, int lc, int ld, size_t smem_limit
   g.NEF = g.NE * g.NF;
   g.n = (la + lb + lc + ld) / 2 + 1;
   g.tsz = (g.LAB + 1) * (g.LCD + 1);
+  int o = 0;
+  g.off_ecomp = o; o += g.NE;
+  g.off_fcomp = o; o += g.NF;
+  g.off_brow = o; o += g.na * g.nb * kMaxTerms;   // row of (e0| for (a, b, term)
+  g.off_bexp = o; o += g.nb * kMaxTerms;          // packed (A-B) exponents | binomial
+  g.off_krow = o; o += g.nc * g.nd * kMaxTerms;   // column of |f0) for (c, d, term)
+  g.off_kexp = o; o += g.nd * kMaxTerms;
+  g.class_ints = (o + 3) & ~3;                    // keeps the double region 16-byte aligned
   const int nD = g.na * g.nb + g.nc * g.nd + g.na * g.nc + g.na * g.nd + g.nb * g.nc + g.nb * g.nd;
   const int nacc = g.nc * g.nd + g.nb * g.nc + g.nb * g.nd;
-  const int nO = g.nb * g.nc * g.nd;
-  const int ntmp = g.nb * g.NF;
   for (int nbt = 32; nbt >= 1; nbt >>= 1) {
     for (int gglob = 0; gglob <= 1; ++gglob) {
       g.nbt = nbt;
       g.G_in_global = gglob;
-      int o = 0;
-      g.off_tab = o; o += nbt * 3 * g.tsz;
-      g.off_G = o; o += gglob ? 0 : g.NEF;
-      g.off_tmp = o; o += ntmp;
-      g.off_O = o; o += nO;
-      g.off_D = o; o += nD;
-      g.off_acc = o; o += nacc;
-      g.per_warp = (o + 1) & ~1;  // keep 16-byte alignment between warps
-      if ((size_t)g.per_warp * 8 * warps <= smem_limit) return g;
+      int w = 0;
+      g.off_tab = w; w += nbt * 3 * g.tsz;
+      g.off_G = w; w += gglob ? 0 : g.NEF;
+      g.off_tmp = w; w += g.nb * g.NF;
+      g.off_O = w; w += g.nb * g.nc * g.nd;
+      g.off_D = w; w += nD;
+      g.off_acc = w; w += nacc;
+      g.off_bcoef = w; w += g.nb * kMaxTerms;
+      g.off_kcoef = w; w += g.nd * kMaxTerms;
+      g.per_warp = (w + 1) & ~1;
+      if (g.smem_bytes(warps) <= smem_limit) return g;
     }
   }
   g.per_warp = -1;
@@ -79,7 +97,6 @@ __device__ __forceinline__ void vrr_item(const GenericGeom& g, double* __restric
                                          double wp, const double PA[3], const double QC[3],
                                          const double PQ[3], double rz, double re, double hz,
                                          double he, double hinv) {
-  // rz = eta/(zeta+eta), re = zeta/(zeta+eta), hz = 0.5/zeta, he = 0.5/eta, hinv = 0.5/(zeta+eta)
   const double b00 = hinv * u;
   const double b10 = hz - hz * rz * u;
   const double b01 = he - he * re * u;
@@ -102,14 +119,91 @@ __device__ __forceinline__ void vrr_item(const GenericGeom& g, double* __restric
   }
 }
 
+// Class tables: component lists and the transfer terms.  brow[(a*nb+b)*T + m] is
+// the row in (e0| of a+k for the m-th shift k <= b (-1 past the last term);
+// bexp[b*T + m] packs the exponents of (A-B) with the binomial product in the
+// high bits.  krow / kexp are the same for the ket.
+__device__ void build_class_tables(const GenericGeom& g, int* __restrict__ ci) {
+  int* ecomp = ci + g.off_ecomp;
+  int* fcomp = ci + g.off_fcomp;
+  int* brow = ci + g.off_brow;
+  int* bexp = ci + g.off_bexp;
+  int* krow = ci + g.off_krow;
+  int* kexp = ci + g.off_kexp;
+  for (int i = threadIdx.x; i < g.NE; i += blockDim.x) {
+    int l = g.la, r = i;
+    while (r >= ncart(l)) { r -= ncart(l); ++l; }
+    ecomp[i] = cart_comp(l, r);
+  }
+  for (int i = threadIdx.x; i < g.NF; i += blockDim.x) {
+    int l = g.lc, r = i;
+    while (r >= ncart(l)) { r -= ncart(l); ++l; }
+    fcomp[i] = cart_comp(l, r);
+  }
+  for (int side = 0; side < 2; ++side) {
+    const int lt = side ? g.ld : g.lb;
+    const int nt = side ? g.nd : g.nb;
+    int* ex = side ? kexp : bexp;
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+      const int cb = cart_comp(lt, i);
+      int m = 0;
+      for (int kx = 0; kx <= comp_x(cb); ++kx)
+        for (int ky = 0; ky <= comp_y(cb); ++ky)
+          for (int kz = 0; kz <= comp_z(cb); ++kz, ++m) {
+            const int bi = (int)(binom(comp_x(cb), kx) * binom(comp_y(cb), ky) * binom(comp_z(cb), kz));
+            ex[i * kMaxTerms + m] = (comp_x(cb) - kx) | ((comp_y(cb) - ky) << 4) |
+                                    ((comp_z(cb) - kz) << 8) | (bi << 12);
+          }
+      for (; m < kMaxTerms; ++m) ex[i * kMaxTerms + m] = -1;
+    }
+  }
+  for (int side = 0; side < 2; ++side) {
+    const int l1 = side ? g.lc : g.la, l2 = side ? g.ld : g.lb;
+    const int n1 = ncart(l1), n2 = ncart(l2);
+    int* rows = side ? krow : brow;
+    for (int i = threadIdx.x; i < n1 * n2; i += blockDim.x) {
+      const int a = i / n2, b = i - a * n2;
+      const int ca = cart_comp(l1, a), cb = cart_comp(l2, b);
+      int m = 0;
+      for (int kx = 0; kx <= comp_x(cb); ++kx)
+        for (int ky = 0; ky <= comp_y(cb); ++ky)
+          for (int kz = 0; kz <= comp_z(cb); ++kz, ++m) {
+            const int ex = comp_x(ca) + kx, ey = comp_y(ca) + ky, ez = comp_z(ca) + kz;
+            rows[i * kMaxTerms + m] = ncart_before(l1, ex + ey + ez) + cart_index(ex, ey, ez);
+          }
+      for (; m < kMaxTerms; ++m) rows[i * kMaxTerms + m] = -1;
+    }
+  }
+}
+
+__device__ __forceinline__ double pow_small(double x, int m) {
+  double r = 1.0;
+  for (int i = 0; i < m; ++i) r *= x;
+  return r;
+}
+
+__device__ __forceinline__ double comp_norm(int c) {
+  return rsqrt(dfact_odd(comp_x(c)) * dfact_odd(comp_y(c)) * dfact_odd(comp_z(c)));
+}
+
 __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKArgs args,
                                                           RysTablesView tab, GenericGeom g,
                                                           double* __restrict__ gscratch) {
   extern __shared__ double smem[];
+  int* ci = reinterpret_cast<int*>(smem);
+  build_class_tables(g, ci);
+  __syncthreads();
+  const int* ecomp = ci + g.off_ecomp;
+  const int* fcomp = ci + g.off_fcomp;
+  const int* brow = ci + g.off_brow;
+  const int* bexp = ci + g.off_bexp;
+  const int* krow = ci + g.off_krow;
+  const int* kexp = ci + g.off_kexp;
+
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps_blk = blockDim.x >> 5;
-  double* ws = smem + (size_t)warp * g.per_warp;
+  double* ws = smem + (size_t)g.class_ints / 2 + (size_t)warp * g.per_warp;
   double* tabs = ws + g.off_tab;
   const int64_t gwarp = (int64_t)blockIdx.x * nwarps_blk + warp;
   const int64_t nwarps = (int64_t)gridDim.x * nwarps_blk;
@@ -125,14 +219,17 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
   double* Akl = ws + g.off_acc;
   double* Ajk = Akl + g.nc * g.nd;
   double* Ajl = Ajk + g.nb * g.nc;
+  double* bcoef = ws + g.off_bcoef;
+  double* kcoef = ws + g.off_kcoef;
 
   const int Kab = blk.bra.Ka * blk.bra.Kb;
   const int Kcd = blk.ket.Ka * blk.ket.Kb;
   const int nitems = Kab * Kcd * g.n;
   const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
   const int W = g.LCD + 1;
+  const int ncd = g.nc * g.nd;
+  const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
 
-  // each warp owns a contiguous run of quartets: one search, then p advances
   const int64_t nq_all = blk.total - blk.t_begin;
   const int64_t per = (nq_all + nwarps - 1) / nwarps;
   const int64_t tbeg = blk.t_begin + gwarp * per;
@@ -140,7 +237,6 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
   int p = -1;
   for (int64_t t = tbeg; t < tend; ++t) {
     const int64_t tl = t - blk.t_begin;
-    // ---- locate the quartet ----
     if (p < 0) {
       if (lane == 0) p = find_bra(blk.offsets, nbra, t);
       p = __shfl_sync(0xffffffffu, p, 0);
@@ -155,79 +251,86 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
     const int fa = __ldg(blk.bra.func_a + p), fb = __ldg(blk.bra.func_b + p);
     const int fc = __ldg(blk.ket.func_a + q), fd = __ldg(blk.ket.func_b + q);
 
-    // ---- (e0|f0) accumulation, in passes of 32*kRmax entries ----
-    for (int pass0 = 0; pass0 < g.NEF; pass0 += 32 * kRmax) {
-      double acc[kRmax];
-      int offs[kRmax];
-#pragma unroll
-      for (int m = 0; m < kRmax; ++m) {
-        acc[m] = 0.0;
-        const int idx = pass0 + lane + 32 * m;
-        int packed = -1;
-        if (idx < g.NEF) {
-          const int ie = idx / g.NF, jf = idx - ie * g.NF;
-          // component of entry ie within shells la..la+lb, jf within lc..lc+ld
-          int le = g.la, r = ie;
-          while (r >= ncart(le)) { r -= ncart(le); ++le; }
-          int lf = g.lc, s = jf;
-          while (s >= ncart(lf)) { s -= ncart(lf); ++lf; }
-          const int ce = cart_comp(le, r), cf = cart_comp(lf, s);
-          const int ox = comp_x(ce) * W + comp_x(cf);
-          const int oy = comp_y(ce) * W + comp_y(cf);
-          const int oz = comp_z(ce) * W + comp_z(cf);
-          packed = ox | (oy << 10) | (oz << 20);
-        }
-        offs[m] = packed;
+    // transfer coefficients of this quartet
+    for (int i = lane; i < g.nb * kMaxTerms; i += 32) {
+      const int e = bexp[i];
+      bcoef[i] = e < 0 ? 0.0 : double(e >> 12) * pow_small(AB[0], e & 15) *
+                                   pow_small(AB[1], (e >> 4) & 15) * pow_small(AB[2], (e >> 8) & 15);
+    }
+    for (int i = lane; i < g.nd * kMaxTerms; i += 32) {
+      const int e = kexp[i];
+      kcoef[i] = e < 0 ? 0.0 : double(e >> 12) * pow_small(CD[0], e & 15) *
+                                   pow_small(CD[1], (e >> 4) & 15) * pow_small(CD[2], (e >> 8) & 15);
+    }
+    for (int i = lane; i < g.NEF; i += 32) G[i] = 0.0;
+    __syncwarp();
+
+    // ---- (e0|f0) accumulation ----
+    unsigned int nprim_done = 0;
+    for (int it0 = 0; it0 < nitems; it0 += g.nbt) {
+      const int it = it0 + lane;
+      if (lane < g.nbt && it < nitems) {
+        const int pq = it / g.n, r = it - pq * g.n;
+        const int ib = pq / Kcd, ik = pq - ib * Kcd;
+        const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
+        const double* pk = blk.ket.prim + (size_t)ik * nket + q;
+        const double zeta = __ldg(pb + PF_ZETA * sb), eta = __ldg(pk + PF_ZETA * sk);
+        const double hz = __ldg(pb + PF_HZ * sb), he = __ldg(pk + PF_HZ * sk);
+        const double PQ[3] = {__ldg(pb + PF_PX * sb) - __ldg(pk + PF_PX * sk),
+                              __ldg(pb + PF_PY * sb) - __ldg(pk + PF_PY * sk),
+                              __ldg(pb + PF_PZ * sb) - __ldg(pk + PF_PZ * sk)};
+        const double PA[3] = {__ldg(pb + PF_PAX * sb), __ldg(pb + PF_PAY * sb), __ldg(pb + PF_PAZ * sb)};
+        const double QC[3] = {__ldg(pk + PF_PAX * sk), __ldg(pk + PF_PAY * sk), __ldg(pk + PF_PAZ * sk)};
+        const double skip =
+            (__ldg(pb + PF_Q * sb) * __ldg(pk + PF_Q * sk) < args.prim_eps) ? 0.0 : 1.0;
+        const double cab = __ldg(pb + PF_C * sb) * skip, ccd = __ldg(pk + PF_C * sk);
+        const double s = zeta + eta;
+        const double rs = rsqrt(s);
+        const double inv = rs * rs;
+        const double rz = eta * inv, re = zeta * inv;
+        const double T = zeta * rz * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+        double u, w;
+        rys_root_one<double>(g.n, r, T, tab, u, w);
+        vrr_item(g, tabs + lane * 3 * g.tsz, u, w * cab * ccd * rs, PA, QC, PQ, rz, re, hz, he,
+                 0.5 * inv);
+        if (r == 0 && skip != 0.0) ++nprim_done;
       }
-      for (int it0 = 0; it0 < nitems; it0 += g.nbt) {
-        const int it = it0 + lane;
-        if (lane < g.nbt && it < nitems) {
-          const int pq = it / g.n, r = it - pq * g.n;
-          const int ib = pq / Kcd, ik = pq - ib * Kcd;
-          const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
-          const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
-          const double* pk = blk.ket.prim + (size_t)ik * nket + q;
-          const double zeta = __ldg(pb + PF_ZETA * sb), eta = __ldg(pk + PF_ZETA * sk);
-          const double hz = __ldg(pb + PF_HZ * sb), he = __ldg(pk + PF_HZ * sk);
-          const double P[3] = {__ldg(pb + PF_PX * sb), __ldg(pb + PF_PY * sb), __ldg(pb + PF_PZ * sb)};
-          const double Qc[3] = {__ldg(pk + PF_PX * sk), __ldg(pk + PF_PY * sk), __ldg(pk + PF_PZ * sk)};
-          const double PA[3] = {__ldg(pb + PF_PAX * sb), __ldg(pb + PF_PAY * sb), __ldg(pb + PF_PAZ * sb)};
-          const double QC[3] = {__ldg(pk + PF_PAX * sk), __ldg(pk + PF_PAY * sk), __ldg(pk + PF_PAZ * sk)};
-          const double cab = __ldg(pb + PF_C * sb), ccd = __ldg(pk + PF_C * sk);
-          const double s = zeta + eta;
-          const double rs = rsqrt(s);
-          const double inv = rs * rs;
-          const double rz = eta * inv, re = zeta * inv;
-          const double PQ[3] = {P[0] - Qc[0], P[1] - Qc[1], P[2] - Qc[2]};
-          const double T = zeta * rz * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-          double u, w;
-          rys_root_one<double>(g.n, r, T, tab, u, w);
-          vrr_item(g, tabs + lane * 3 * g.tsz, u, w * cab * ccd * rs, PA, QC, PQ, rz, re, hz, he,
-                   0.5 * inv);
-        }
-        __syncwarp();
-        const int nb_now = min(g.nbt, nitems - it0);
+      __syncwarp();
+      const int nb_now = min(g.nbt, nitems - it0);
+      for (int base = 0; base < g.NEF; base += 32 * kR) {
+        double acc[kR];
+        int off[kR];
 #pragma unroll
-        for (int m = 0; m < kRmax; ++m) {
-          const int pk = offs[m];
-          if (pk >= 0) {
-            const int ox = pk & 1023, oy = (pk >> 10) & 1023, oz = pk >> 20;
-            double a = acc[m];
-            for (int sidx = 0; sidx < nb_now; ++sidx) {
-              const double* T3 = tabs + sidx * 3 * g.tsz;
-              a += T3[ox] * T3[g.tsz + oy] * T3[2 * g.tsz + oz];
-            }
-            acc[m] = a;
+        for (int m = 0; m < kR; ++m) {
+          const int idx = base + lane + 32 * m;
+          acc[m] = 0.0;
+          off[m] = -1;
+          if (idx < g.NEF) {
+            const int ie = idx / g.NF, jf = idx - ie * g.NF;
+            const int ce = ecomp[ie], cf = fcomp[jf];
+            off[m] = (comp_x(ce) * W + comp_x(cf)) | ((comp_y(ce) * W + comp_y(cf)) << 10) |
+                     ((comp_z(ce) * W + comp_z(cf)) << 20);
           }
         }
-        __syncwarp();
-      }
+        for (int sidx = 0; sidx < nb_now; ++sidx) {
+          const double* T3 = tabs + sidx * 3 * g.tsz;
 #pragma unroll
-      for (int m = 0; m < kRmax; ++m) {
-        const int idx = pass0 + lane + 32 * m;
-        if (idx < g.NEF) G[idx] = acc[m];
+          for (int m = 0; m < kR; ++m) {
+            const int o = off[m];
+            if (o >= 0)
+              acc[m] += T3[o & 1023] * T3[g.tsz + ((o >> 10) & 1023)] * T3[2 * g.tsz + (o >> 20)];
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < kR; ++m) {
+          const int idx = base + lane + 32 * m;
+          if (idx < g.NEF) G[idx] += acc[m];
+        }
       }
+      __syncwarp();
     }
+
+    count_prims(args.prim_count, nprim_done);
 
     // ---- digestion setup ----
     const double sym = quartet_weight(blk, p, q);
@@ -237,7 +340,7 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
         const int a = i / g.nb, b = i - a * g.nb;
         Dij[i] = __ldg(args.D + (size_t)(fa + a) * nbf + fb + b);
       }
-      for (int i = lane; i < g.nc * g.nd; i += 32) {
+      for (int i = lane; i < ncd; i += 32) {
         const int c = i / g.nd, d = i - c * g.nd;
         Dkl[i] = __ldg(args.D + (size_t)(fc + c) * nbf + fd + d);
         Akl[i] = 0.0;
@@ -264,48 +367,35 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
     double smax = 0.0;
     __syncwarp();
 
-    // ---- per bra component a: HRR into O[b][c][d], then digest ----
-    const int ncd = g.nc * g.nd;
     for (int a = 0; a < g.na; ++a) {
-      const int ca = cart_comp(g.la, a);
-      // bra transfer: tmp[b][f] = sum_k C(b,k) AB^(b-k) G[a+k][f]
+      // bra transfer: tmp[b][f] = sum_m bcoef[b][m] G[brow[a][b][m]][f]
       for (int i = lane; i < g.nb * g.NF; i += 32) {
         const int b = i / g.NF, f = i - b * g.NF;
-        const int cb = cart_comp(g.lb, b);
-        const int bx = comp_x(cb), by = comp_y(cb), bz = comp_z(cb);
+        const int* rows = brow + (a * g.nb + b) * kMaxTerms;
+        const double* cf = bcoef + b * kMaxTerms;
         double v = 0.0;
-        for (int kx = 0; kx <= bx; ++kx)
-          for (int ky = 0; ky <= by; ++ky)
-            for (int kz = 0; kz <= bz; ++kz) {
-              const int ex = comp_x(ca) + kx, ey = comp_y(ca) + ky, ez = comp_z(ca) + kz;
-              const int le = ex + ey + ez;
-              const int row = ncart_before(g.la, le) + cart_index(ex, ey, ez);
-              const double cf = binom(bx, kx) * binom(by, ky) * binom(bz, kz) *
-                                ipow(AB[0], bx - kx) * ipow(AB[1], by - ky) * ipow(AB[2], bz - kz);
-              v += cf * G[row * g.NF + f];
-            }
+        for (int m = 0; m < kMaxTerms; ++m) {
+          const int row = rows[m];
+          if (row < 0) break;
+          v += cf[m] * G[row * g.NF + f];
+        }
         tmp[i] = v;
       }
       __syncwarp();
-      // ket transfer + normalization: O[b][c][d]
-      const double na_f = norm_factor(g.la, a);
+      const double na_f = comp_norm(cart_comp(g.la, a));
       for (int i = lane; i < g.nb * ncd; i += 32) {
         const int b = i / ncd, cdi = i - b * ncd;
         const int c = cdi / g.nd, d = cdi - c * g.nd;
-        const int cc = cart_comp(g.lc, c), cdd = cart_comp(g.ld, d);
-        const int dx = comp_x(cdd), dy = comp_y(cdd), dz = comp_z(cdd);
+        const int* cols = krow + cdi * kMaxTerms;
+        const double* cf = kcoef + d * kMaxTerms;
         double v = 0.0;
-        for (int kx = 0; kx <= dx; ++kx)
-          for (int ky = 0; ky <= dy; ++ky)
-            for (int kz = 0; kz <= dz; ++kz) {
-              const int fx = comp_x(cc) + kx, fy = comp_y(cc) + ky, fz = comp_z(cc) + kz;
-              const int lf = fx + fy + fz;
-              const int col = ncart_before(g.lc, lf) + cart_index(fx, fy, fz);
-              const double cf = binom(dx, kx) * binom(dy, ky) * binom(dz, kz) *
-                                ipow(CD[0], dx - kx) * ipow(CD[1], dy - ky) * ipow(CD[2], dz - kz);
-              v += cf * tmp[b * g.NF + col];
-            }
-        v *= na_f * norm_factor(g.lb, b) * norm_factor(g.lc, c) * norm_factor(g.ld, d);
+        for (int m = 0; m < kMaxTerms; ++m) {
+          const int col = cols[m];
+          if (col < 0) break;
+          v += cf[m] * tmp[b * g.NF + col];
+        }
+        v *= na_f * comp_norm(cart_comp(g.lb, b)) * comp_norm(cart_comp(g.lc, c)) *
+             comp_norm(cart_comp(g.ld, d));
         O[i] = v;
         if (args.mode == MODE_RAW) {
           args.raw_out[(size_t)tl * g.na * g.nb * ncd + (size_t)a * g.nb * ncd + i] = v;
@@ -316,7 +406,6 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
       __syncwarp();
       if (args.mode == MODE_JK) {
         const int nbf = args.nbf;
-        // targets of this tile
         for (int i = lane; i < g.nb + g.nc + g.nd; i += 32) {
           if (i < g.nb) {  // J_ij[a][b] += 2 s sum_cd O[b][c][d] D_kl[c][d]
             const int b = i;
@@ -337,19 +426,18 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
             atomicAdd(args.K + (size_t)(fa + a) * nbf + fd + d, sym * v);
           }
         }
-        // accumulators across tiles
-        for (int i = lane; i < ncd; i += 32) {  // J_kl[c][d] += 2 s sum_b O[b][c][d] D_ij[a][b]
+        for (int i = lane; i < ncd; i += 32) {  // J_kl[c][d] partial: sum_b O D_ij[a][b]
           double v = 0.0;
           for (int b = 0; b < g.nb; ++b) v += O[b * ncd + i] * Dij[a * g.nb + b];
           Akl[i] += v;
         }
-        for (int i = lane; i < g.nb * g.nc; i += 32) {  // K_jk[b][c] += s sum_d O D_il[a][d]
+        for (int i = lane; i < g.nb * g.nc; i += 32) {  // K_jk[b][c] partial: sum_d O D_il[a][d]
           const int b = i / g.nc, c = i - b * g.nc;
           double v = 0.0;
           for (int d = 0; d < g.nd; ++d) v += O[b * ncd + c * g.nd + d] * Dil[a * g.nd + d];
           Ajk[i] += v;
         }
-        for (int i = lane; i < g.nb * g.nd; i += 32) {  // K_jl[b][d] += s sum_c O D_ik[a][c]
+        for (int i = lane; i < g.nb * g.nd; i += 32) {  // K_jl[b][d] partial: sum_c O D_ik[a][c]
           const int b = i / g.nd, d = i - b * g.nd;
           double v = 0.0;
           for (int c = 0; c < g.nc; ++c) v += O[b * ncd + c * g.nd + d] * Dik[a * g.nc + c];
@@ -396,10 +484,9 @@ int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesV
   GenericGeom g = make_geom(la, lb, lc, ld, smem_max, warps);
   if (g.per_warp < 0) { warps = 1; g = make_geom(la, lb, lc, ld, smem_max, warps); }
   if (g.per_warp < 0) return -1;
-  const size_t smem = (size_t)g.per_warp * 8 * warps;
-  // enough warps to cover the SMs several times; grid-stride inside
-  int64_t want = (blk.total - blk.t_begin + warps - 1) / warps;
-  int64_t cap = (int64_t)num_sms * 16;
+  const size_t smem = g.smem_bytes(warps);
+  const int64_t want = (blk.total - blk.t_begin + warps - 1) / warps;
+  const int64_t cap = (int64_t)num_sms * 8;
   int grid = (int)(want < cap ? want : cap);
   if (g.G_in_global) {
     const size_t need = (size_t)grid * warps * g.NEF;
@@ -410,8 +497,9 @@ int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesV
   }
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(eri_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem_max);
+    if (cudaFuncSetAttribute(eri_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_max) != cudaSuccess)
+      return -3;
     attr_set = true;
   }
   eri_generic_kernel<<<grid, warps * 32, smem, stream>>>(blk, args, tab, g, gscratch);
@@ -419,11 +507,11 @@ int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesV
 }
 
 size_t generic_global_scratch_doubles(int la, int lb, int lc, int ld, int num_sms) {
-  GenericGeom g = make_geom(la, lb, lc, ld, 227 * 1024, 4);
   int warps = 4;
-  if (g.per_warp < 0) { warps = 1; g = make_geom(la, lb, lc, ld, 227 * 1024, 1); }
+  GenericGeom g = make_geom(la, lb, lc, ld, 227 * 1024, warps);
+  if (g.per_warp < 0) { warps = 1; g = make_geom(la, lb, lc, ld, 227 * 1024, warps); }
   if (g.per_warp < 0 || !g.G_in_global) return 0;
-  return (size_t)num_sms * 16 * warps * g.NEF;
+  return (size_t)num_sms * 8 * warps * g.NEF;
 }
 
 }  // namespace lai

@@ -66,8 +66,14 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 #pragma unroll
   for (int i = 0; i < NK * NF; ++i) G[i] = R(0);
 
+  const double peps = args.prim_eps;
+  unsigned int nprim_done = 0;
   for (int ib = 0; ib < Kab; ++ib) {
     const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
+    // primitive pairs are sorted by their Schwarz bound: once the bra bound times
+    // the largest ket bound of the class drops below the cut, the rest do too
+    const double qab = __ldg(pb + PF_Q * sb);
+    if (qab * blk.ket.qprim_max < peps) break;
     const R zeta = R(__ldg(pb + PF_ZETA * sb));
     const R hz = R(__ldg(pb + PF_HZ * sb));
     const R Px = R(__ldg(pb + PF_PX * sb)), Py = R(__ldg(pb + PF_PY * sb)), Pz = R(__ldg(pb + PF_PZ * sb));
@@ -76,6 +82,8 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
     const R cab = R(__ldg(pb + PF_C * sb));
     for (int ik = 0; ik < Kcd; ++ik) {
       const double* pk = blk.ket.prim + (size_t)ik * nket + q;
+      if (qab * __ldg(pk + PF_Q * sk) < peps) break;  // sorted: the rest are smaller
+      ++nprim_done;
       const R eta = R(__ldg(pk + PF_ZETA * sk));
       const R he = R(__ldg(pk + PF_HZ * sk));
       const R PQx = Px - R(__ldg(pk + PF_PX * sk));
@@ -142,6 +150,8 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
       }
     }
   }
+
+  count_prims(args.prim_count, (active && a == 0) ? nprim_done : 0u);
 
   // ---- transfer: H[b][f] = sum_{k<=b} C(b,k) AB^(b-k) G[k][f]; V[b][c][d] ----
   const double ABx = __ldg(blk.bra.AB + p), ABy = __ldg(blk.bra.AB + nbra + p),

@@ -35,6 +35,8 @@ enum PrimField : int {
   PF_PX, PF_PY, PF_PZ,     // Gaussian product centre P
   PF_PAX, PF_PAY, PF_PAZ,  // P - A
   PF_C,          // sqrt(2) pi^{5/4} c_a c_b exp(-alpha_a alpha_b |AB|^2 / zeta) / zeta
+  PF_Q,          // primitive Schwarz bound sqrt(max |(a_p b_q|a_p b_q)|); primitive pairs
+                 // of each shell pair are stored in descending PF_Q order
   PF_COUNT
 };
 
@@ -49,6 +51,7 @@ struct PairClassDev {
   const double* Q;     // [npairs] Schwarz bound, descending
   const double* AB;    // [3 * npairs] A - B, SoA
   const double* prim;  // [PF_COUNT * Ka*Kb * npairs]
+  double qprim_max;    // largest PF_Q of the class
 };
 
 // One launch: the canonical quartets (p, q) with p a pair of class `bra` and q a

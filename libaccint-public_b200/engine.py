@@ -87,7 +87,8 @@ class FockBuilder:
 
 
 class Engine:
-    def __init__(self, basis, threshold=1e-12, device=0):
+    def __init__(self, basis, threshold=1e-12, device=0, prim_threshold=None):
+        """``prim_threshold``: primitive-quartet cut (None = 1e-3 * threshold, 0 = off)."""
         self.basis = basis
         self.threshold = threshold
         L = _lib.lib()
@@ -95,6 +96,8 @@ class Engine:
         L.lai_engine_opts_default(ctypes.byref(opts))
         opts.schwarz_threshold = threshold
         opts.device = device
+        if prim_threshold is not None:
+            opts.prim_threshold = prim_threshold
         h = ctypes.c_void_p()
         _lib.check(L.lai_engine_create(basis.handle(), ctypes.byref(opts), ctypes.byref(h)))
         self._h = h
@@ -146,17 +149,21 @@ class Engine:
         return rep
 
     def last_profile(self):
-        """Per-launch (ms, alg_flops, quartets, (la,lb,lc,ld)) of the last profiled build."""
+        """Per-launch profile of the last build made with profile=True: dict of arrays
+        ms, alg_flops (all nonzero primitives), alg_flops_executed (primitive
+        quartets that passed the primitive cut), quartets, prim_quartets, lclass."""
         L = _lib.lib()
-        n = L.lai_jk_last_profile(self._h, 0, None, None, None, None)
-        ms = np.zeros(n)
-        fl = np.zeros(n)
-        nq = np.zeros(n, dtype=np.int64)
-        lc = np.zeros(4 * n, dtype=np.int32)
-        got = L.lai_jk_last_profile(self._h, n, ms.ctypes.data, fl.ctypes.data, nq.ctypes.data, lc.ctypes.data)
+        n = L.lai_jk_last_profile(self._h, 0, None, None, None, None, None, None)
+        out = {"ms": np.zeros(n), "alg_flops": np.zeros(n), "alg_flops_executed": np.zeros(n),
+               "quartets": np.zeros(n, dtype=np.int64), "prim_quartets": np.zeros(n, dtype=np.int64),
+               "lclass": np.zeros(4 * n, dtype=np.int32)}
+        got = L.lai_jk_last_profile(self._h, n, *(out[k].ctypes.data for k in
+                                                  ("ms", "alg_flops", "alg_flops_executed", "quartets",
+                                                   "prim_quartets", "lclass")))
         if got < 0:
             _lib.check(got)
-        return ms, fl, nq, lc.reshape(-1, 4)
+        out["lclass"] = out["lclass"].reshape(-1, 4)
+        return out
 
     def quartet_count(self):
         return int(_lib.lib().lai_engine_quartet_count(self._h))

@@ -193,3 +193,16 @@ def test_nonsymmetric_density_rejected_when_checked(lai):
     D[0, 1] += 1e-3
     with pytest.raises(lai.LibAccIntError):
         e.jk(D, check_symmetric=True)
+
+
+def test_primitive_screening_is_within_tolerance(lai):
+    """Primitive-quartet screening (q_ab q_cd < 1e-3 * threshold) changes J/K by
+    far less than the 1e-10 parity bar: compare with the cut switched off."""
+    w = lai.workloads.make("h2o8_ccpvdz")
+    e_on = lai.Engine(w.basis, threshold=1e-12)
+    e_off = lai.Engine(w.basis, threshold=1e-12, prim_threshold=0.0)
+    J1, K1, r1 = e_on.jk(w.D)
+    J0, K0, r0 = e_off.jk(w.D)
+    assert r1.quartets_fp64 == r0.quartets_fp64
+    assert np.max(np.abs(J1 - J0)) < 1e-11
+    assert np.max(np.abs(K1 - K0)) < 1e-11
