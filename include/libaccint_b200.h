@@ -137,6 +137,22 @@ LAI_API int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double
 LAI_API int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d_J, double* d_K,
                         void* stream, const lai_jk_opts* opts, lai_jk_report* report);
 
+/* J/K build that allocates nothing when called (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc at this point: code
+ * recording a CUDA graph, plugins whose host application owns the whole device
+ * through its own allocator, real-time drivers that forbid allocation after
+ * start-up.  Same result as lai_jk_build_device(); the two nbf x nbf
+ * accumulators live in a fixed 4 MiB array of the library's device image
+ * (held on every GPU that loads the library until exit), hence
+ * nbf <= LAI_NOALLOC_MAX_NBF, else LAI_EINVAL; bases with a class whose
+ * integral block needs global scratch give LAI_ENOTSUP.  All calls share the
+ * array: calls whose device work overlaps race.  The first call on a device
+ * looks up the array's address -- make it before any stream capture.
+ * Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream). */
+#define LAI_NOALLOC_MAX_NBF 512
+LAI_API int lai_jk_build_noalloc(lai_engine* engine, const double* d_D, double* d_J, double* d_K,
+                                 void* stream);
+
 /* ---------------------------------------------------------------------------
  * Raw integrals of every canonical shell quartet that passes the engine's
  * Schwarz threshold.  Replaces Engine::compute_batch_screened(op, screening)

@@ -20,7 +20,7 @@ EXPORTED = [
     "lai_engine_opts_default", "lai_engine_create", "lai_engine_destroy", "lai_engine_schwarz",
     "lai_jk_opts_default", "lai_jk_build", "lai_jk_build_device", "lai_eri_batch_screened",
     "lai_jk_last_profile", "lai_engine_sample_quartets", "lai_engine_quartet_count",
-    "lai_probe_fp64_peak",
+    "lai_probe_fp64_peak", "lai_jk_build_noalloc",
 ]
 
 
@@ -85,6 +85,7 @@ def lib():
         "lai_engine_sample_quartets": (I, [P, ctypes.c_int64, ctypes.c_uint64, P]),
         "lai_engine_quartet_count": (ctypes.c_int64, [P]),
         "lai_probe_fp64_peak": (I, [I, ctypes.POINTER(ctypes.c_double)]),
+        "lai_jk_build_noalloc": (I, [P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -969,3 +969,19 @@ int lai_probe_fp64_peak(int device, double* tflops) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Read-only accessors for other translation units of the library (not C ABI).
+// ---------------------------------------------------------------------------
+namespace lai {
+
+int engine_device(const lai_engine* E) { return E->device; }
+int engine_num_sms(const lai_engine* E) { return E->num_sms; }
+int engine_nbf(const lai_engine* E) { return (int)E->basis->nbf; }
+double engine_prim_eps(const lai_engine* E) { return E->prim_eps; }
+RysTablesView engine_tables(const lai_engine* E) { return E->tab; }
+int engine_block_count(const lai_engine* E) { return (int)E->blocks.size(); }
+QuartetBlock engine_block(const lai_engine* E, int i) { return make_block(E, *E->blocks[i]); }
+void engine_set_error(const char* msg) { g_last_error = msg; }
+
+}  // namespace lai
