@@ -97,6 +97,25 @@ struct JKArgs {
   unsigned long long* prim_count;  // optional: += primitive quartets executed by the launch
 };
 
+// One ket primitive pair's data, loaded a loop iteration ahead of its use so the
+// global-memory latency overlaps the previous primitive's arithmetic (fields a
+// class never reads are removed by the compiler).
+struct KetPrim {
+  double q, eta, he, px, py, pz, qcx, qcy, qcz, c;
+};
+__device__ __forceinline__ void load_ket_prim(const double* __restrict__ pk, size_t sk, KetPrim& k) {
+  k.q = __ldg(pk + PF_Q * sk);
+  k.eta = __ldg(pk + PF_ZETA * sk);
+  k.he = __ldg(pk + PF_HZ * sk);
+  k.px = __ldg(pk + PF_PX * sk);
+  k.py = __ldg(pk + PF_PY * sk);
+  k.pz = __ldg(pk + PF_PZ * sk);
+  k.qcx = __ldg(pk + PF_PAX * sk);
+  k.qcy = __ldg(pk + PF_PAY * sk);
+  k.qcz = __ldg(pk + PF_PAZ * sk);
+  k.c = __ldg(pk + PF_C * sk);
+}
+
 // Add a per-lane count to a launch counter (one atomic per warp).
 __device__ __forceinline__ void count_prims(unsigned long long* ctr, unsigned int n) {
   if (!ctr) return;

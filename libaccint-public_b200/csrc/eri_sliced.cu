@@ -16,6 +16,7 @@
 // (compile-time-indexed registers) instead of indexing them at run time.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "eri_device.cuh"
@@ -80,18 +81,21 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
     const R PAx = R(__ldg(pb + PF_PAX * sb)), PAy = R(__ldg(pb + PF_PAY * sb)),
             PAz = R(__ldg(pb + PF_PAZ * sb));
     const R cab = R(__ldg(pb + PF_C * sb));
+    const double* pk0 = blk.ket.prim + q;
+    KetPrim nxt;
+    load_ket_prim(pk0, sk, nxt);
     for (int ik = 0; ik < Kcd; ++ik) {
-      const double* pk = blk.ket.prim + (size_t)ik * nket + q;
-      if (qab * __ldg(pk + PF_Q * sk) < peps) break;  // sorted: the rest are smaller
+      const KetPrim cur = nxt;
+      if (qab * cur.q < peps) break;  // sorted: the rest are smaller
+      if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
       ++nprim_done;
-      const R eta = R(__ldg(pk + PF_ZETA * sk));
-      const R he = R(__ldg(pk + PF_HZ * sk));
-      const R PQx = Px - R(__ldg(pk + PF_PX * sk));
-      const R PQy = Py - R(__ldg(pk + PF_PY * sk));
-      const R PQz = Pz - R(__ldg(pk + PF_PZ * sk));
-      const R QCx = R(__ldg(pk + PF_PAX * sk)), QCy = R(__ldg(pk + PF_PAY * sk)),
-              QCz = R(__ldg(pk + PF_PAZ * sk));
-      const R ccd = R(__ldg(pk + PF_C * sk));
+      const R eta = R(cur.eta);
+      const R he = R(cur.he);
+      const R PQx = Px - R(cur.px);
+      const R PQy = Py - R(cur.py);
+      const R PQz = Pz - R(cur.pz);
+      const R QCx = R(cur.qcx), QCy = R(cur.qcy), QCz = R(cur.qcz);
+      const R ccd = R(cur.c);
       const R s = zeta + eta;
       const R rs = R(1) / sqrt(s);
       const R inv = rs * rs;
@@ -368,7 +372,7 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 
 template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) eri_sliced_kernel(QuartetBlock blk, JKArgs args,
-                                                         RysTablesView tab) {
+                                                         RysTablesView tab, int kSuper) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   constexpr int TW = next_pow2(ncart(LA));
   constexpr int QPW = 32 / TW;  // quartets per warp
@@ -382,16 +386,25 @@ __global__ void __launch_bounds__(128) eri_sliced_kernel(QuartetBlock blk, JKArg
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int nbra = blk.bra.npairs;
-  for (int64_t c = wid; c < nchunks; c += nw) {
-    const int64_t t0 = blk.t_begin + c * QPW;
-    const int64_t t = t0 + slot;
-    const bool active = t < blk.total;
-    const int64_t te = active ? t : blk.total - 1;
-    int p = 0;
-    if (lane == 0) p = find_bra(blk.offsets, nbra, t0);
-    p = __shfl_sync(0xffffffffu, p, 0);
-    while (te >= __ldg(blk.offsets + p + 1)) ++p;
-    sliced_quartet<LA, LB, LC, LD, R>(blk, args, tab, stab, te, p, active, a);
+  const int64_t nsuper = (nchunks + kSuper - 1) / kSuper;
+  for (int64_t sc = wid; sc < nsuper; sc += nw) {
+    const int64_t c1 = min(nchunks, (sc + 1) * kSuper);
+    int pw = -1;
+    for (int64_t c = sc * kSuper; c < c1; ++c) {
+      const int64_t t0 = blk.t_begin + c * QPW;
+      const int64_t t = t0 + slot;
+      const bool active = t < blk.total;
+      const int64_t te = active ? t : blk.total - 1;
+      if (pw < 0) {
+        if (lane == 0) pw = find_bra(blk.offsets, nbra, t0);
+        pw = __shfl_sync(0xffffffffu, pw, 0);
+      } else {
+        while (t0 >= __ldg(blk.offsets + pw + 1)) ++pw;
+      }
+      int p = pw;
+      while (te >= __ldg(blk.offsets + p + 1)) ++p;
+      sliced_quartet<LA, LB, LC, LD, R>(blk, args, tab, stab, te, p, active, a);
+    }
   }
 }
 
@@ -418,7 +431,11 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
   const int64_t want = (nchunks + (threads / 32) - 1) / (threads / 32);
   const int64_t cap = (int64_t)num_sms * per_sm;
   const int grid = (int)(want < cap ? want : cap);
-  kern<<<grid, threads, smem, stream>>>(blk, args, tab);
+  // chunks per super-chunk: long runs (one bra search each) when the launch has
+  // plenty of work, short ones when it would otherwise leave warps idle
+  const int64_t warps_total = (int64_t)grid * (threads / 32);
+  const int ksuper = (int)std::max<int64_t>(1, std::min<int64_t>(16, nchunks / (8 * warps_total)));
+  kern<<<grid, threads, smem, stream>>>(blk, args, tab, ksuper);
   return cudaGetLastError() == cudaSuccess ? 1 : -3;
 }
 

@@ -1,0 +1,16 @@
+// Explicit instantiations of the small-class kernels (part 5 of 6; split so
+// nvcc compiles the classes in parallel).
+#include "eri_small_impl.cuh"
+
+namespace lai {
+namespace small_detail {
+
+template int launch_one<1, 1, 1, 0>(const QuartetBlock&, const JKArgs&, const RysTablesView&,
+                                   cudaStream_t, bool, int);
+template int launch_one<3, 0, 0, 0>(const QuartetBlock&, const JKArgs&, const RysTablesView&,
+                                   cudaStream_t, bool, int);
+template int launch_one<2, 1, 1, 0>(const QuartetBlock&, const JKArgs&, const RysTablesView&,
+                                   cudaStream_t, bool, int);
+
+}  // namespace small_detail
+}  // namespace lai
