@@ -36,6 +36,13 @@ WORKLOAD = "h2o64_ccpvdz"
 METRIC = "jk_quartets_per_s"
 UNIT = "quartets/s"
 
+# DRAM bytes (read + write) per launch of a class kernel, averaged over the launches of
+# one timed step in a one-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum);
+# the capture and its command are summarised under profiles/.
+TRAFFIC_PER_LAUNCH = {
+    ("h2o64_ccpvdz", "(ps|ss)"): 21.41e6,  # profiles/eri_small_psss_h2o64_h2o16.txt
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -278,17 +285,20 @@ def main():
     torch.cuda.synchronize()
     pr = eng.last_profile()
     pms, pfl, pfx, pcl = pr["ms"], pr["alg_flops"], pr["alg_flops_executed"], pr["lclass"]
-    top = int(np.argmax(pms))
     peak = lai.probe_fp64_peak(local)
     roof_all = float(np.sum(pfx) / (np.sum(pms) * 1e-3) / 1e12)
     roof_all_nominal = float(np.sum(pfl) / (np.sum(pms) * 1e-3) / 1e12)
-    dom_tf = float(pfx[top] / (pms[top] * 1e-3) / 1e12)
     by_class = {}
     for ms, fl, cl in zip(pms, pfx, pcl):
         key = "(%s%s|%s%s)" % tuple("spdfg"[x] for x in cl)
-        a = by_class.setdefault(key, [0.0, 0.0])
+        a = by_class.setdefault(key, [0.0, 0.0, 0])
         a[0] += ms
         a[1] += fl
+        a[2] += 1
+    # dominant kernel = the class kernel with the largest share of device time
+    dom_key, (dom_ms, dom_fl, dom_n) = max(by_class.items(), key=lambda kv: kv[1][0])
+    dom_tf = float(dom_fl / (dom_ms * 1e-3) / 1e12)
+    traffic = TRAFFIC_PER_LAUNCH.get((args.workload, dom_key))
     prim_exec = int(np.sum(pr["prim_quartets"]))
 
     out = None
@@ -317,9 +327,10 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n * n,
                     "d2h_bytes_per_step": 16 * n * n, "ms_per_step": et.item() / args.steps},
             "roofline": {"bound": "fp64", "achieved": dom_tf, "peak": peak, "unit": "TFLOP/s",
-                         "frac": dom_tf / peak, "traffic": None,
-                         "kernel": "class %s launch (largest device time, %.1f ms)" % (
-                             "(%s%s|%s%s)" % tuple("spdfg"[x] for x in pcl[top]), pms[top]),
+                         "frac": dom_tf / peak, "traffic": traffic,
+                         "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+                         "kernel": "class %s kernel: %d launches, %.1f ms of the step (largest share)" % (
+                             dom_key, dom_n, dom_ms),
                          "all_kernels_achieved": roof_all, "all_kernels_frac": roof_all / peak,
                          "work": "algorithmic FP64 work of the primitive quartets executed "
                                  "(those passing the primitive Schwarz cut); counting all nonzero "
