@@ -109,7 +109,13 @@ LAI_API int lai_engine_schwarz(lai_engine* engine, double* Q);
  * ------------------------------------------------------------------------- */
 typedef struct {
   double fp32_cut;   /* mixed precision: quartets with Q_ij*Q_kl*max|D| < fp32_cut
-                        run the Rys recursion in FP32 (0 = all FP64)             */
+                        run roots, recurrences and primitive contraction in FP32
+                        (transfer, normalization and J/K digestion stay FP64);
+                        0 = all FP64.  The Schwarz cut fp32_cut/max|D| is rounded
+                        down to a power of two; reading max|D| costs one stream
+                        synchronisation.  No counterpart in the reference, whose
+                        float path computes in FP64 and casts
+                        (include/libaccint/engine/precision_dispatch.hpp:200-259). */
   int check_symmetric; /* 1 = reject a D that is not symmetric to 1e-12 (host)  */
   int shard_index;     /* multi-GPU: this rank computes shard shard_index of     */
   int shard_count;     /* shard_count equal slices of every quartet block (1 = all);
@@ -126,6 +132,7 @@ typedef struct {
   double seconds_device;   /* device time of the integral + digestion kernels */
   double seconds_total;    /* wall time of the call                           */
   int kernel_launches;     /* kernels launched by the call                    */
+  double fp32_schwarz_cut; /* Q_ij*Q_kl below which quartets ran in FP32 (0 = none) */
 } lai_jk_report;
 
 /* Host buffers (nbf*nbf doubles each). report may be NULL. */
@@ -133,7 +140,8 @@ LAI_API int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double
                  const lai_jk_opts* opts, lai_jk_report* report);
 /* Device buffers on the engine's device; stream is a cudaStream_t (NULL = legacy
  * default stream).  Asynchronous: returns after enqueueing (report times are
- * then not filled). */
+ * then not filled), except that opts->fp32_cut > 0 first synchronises the stream
+ * once to read max|D|. */
 LAI_API int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d_J, double* d_K,
                         void* stream, const lai_jk_opts* opts, lai_jk_report* report);
 

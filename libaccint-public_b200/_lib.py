@@ -49,7 +49,8 @@ class QuartetMeta(ctypes.Structure):
 class JKReport(ctypes.Structure):
     _fields_ = [("quartets_fp64", ctypes.c_int64), ("quartets_fp32", ctypes.c_int64),
                 ("alg_flops", ctypes.c_double), ("seconds_device", ctypes.c_double),
-                ("seconds_total", ctypes.c_double), ("kernel_launches", ctypes.c_int)]
+                ("seconds_total", ctypes.c_double), ("kernel_launches", ctypes.c_int),
+                ("fp32_schwarz_cut", ctypes.c_double)]
 
 
 _lib = None

@@ -220,6 +220,12 @@ struct ClassPairBlock {
   double alg_flops = 0;         // per quartet of this block (all nonzero primitives)
   double flops_per_prim = 0;    // per primitive quartet
   double flops_per_quartet = 0; // per contracted quartet (normalization + digestion)
+  // Mixed-precision split of this block for one FP32 cut: the kets of bra pair p
+  // are sorted by Schwarz bound, so those with Q_p Q_q >= cut form a prefix (the
+  // FP64 part, offsets64) and the rest a suffix (the FP32 part: offsets32, with
+  // qbegin32[p] its first ket).
+  int64_t total64 = 0, total32 = 0;
+  DevBuf d_off64, d_off32, d_qb32;
 };
 
 // Algorithmic FP work of one canonical quartet (one unit), the single accounting
@@ -270,6 +276,8 @@ struct lai_engine {
   DevBuf d_scratch;
   size_t scratch_doubles = 0;
   DevBuf d_status;
+  double split_cut = -1.0;       // FP32 cut the blocks' mixed-precision split was built for
+  DevBuf d_absmax;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // per-launch profile of the last build with opts.profile
   std::vector<cudaEvent_t> prof_ev;
@@ -380,16 +388,22 @@ int ensure_scratch(lai_engine* E, size_t doubles) {
   return LAI_OK;
 }
 
-int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs& args) {
+// Launches the kernel of the block's class.  fp32 asks for the FP32 variant; the
+// classes without one (generic kernel) run in FP64, and *ran_fp32 says which ran.
+int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs& args,
+                 bool fp32 = false, bool* ran_fp32 = nullptr) {
   const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
+  if (ran_fp32) *ran_fp32 = false;
   if (lai::small_class_supported(la, lb, lc, ld)) {
-    const int rc = lai::launch_small(blk, args, E->tab, E->stream, false, E->num_sms);
+    const int rc = lai::launch_small(blk, args, E->tab, E->stream, fp32, E->num_sms);
+    if (ran_fp32) *ran_fp32 = fp32;
     if (rc < 0) return fail(LAI_ECUDA, std::string("small-class launch failed: ") +
                                            cudaGetErrorString(cudaGetLastError()));
     return LAI_OK;
   }
   if (lai::sliced_class_supported(la, lb, lc, ld)) {
-    const int rc = lai::launch_sliced(blk, args, E->tab, E->stream, false, E->num_sms);
+    const int rc = lai::launch_sliced(blk, args, E->tab, E->stream, fp32, E->num_sms);
+    if (ran_fp32) *ran_fp32 = fp32;
     if (rc < 0) return fail(LAI_ECUDA, std::string("sliced launch failed: ") +
                                            cudaGetErrorString(cudaGetLastError()));
     return LAI_OK;
@@ -582,6 +596,66 @@ lai::QuartetBlock make_block(const lai_engine* E, const ClassPairBlock& b) {
   return q;
 }
 
+__global__ void absmax_kernel(const double* __restrict__ x, size_t n, unsigned long long* out) {
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(x[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  // non-negative doubles order like their bit patterns
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// max |x_i| of a device array (one stream synchronisation).
+int device_absmax(lai_engine* E, const double* x, size_t n, cudaStream_t stream, double* out) {
+  if (E->d_absmax.bytes < sizeof(unsigned long long)) LAI_CUDA_TRY(E->d_absmax.alloc(sizeof(unsigned long long)));
+  LAI_CUDA_TRY(cudaMemsetAsync(E->d_absmax.p, 0, sizeof(unsigned long long), stream));
+  if (n > 0) {
+    const size_t want = (n + 255) / 256;
+    const unsigned grid = (unsigned)std::min<size_t>(want, (size_t)E->num_sms * 8);
+    absmax_kernel<<<grid, 256, 0, stream>>>(x, n, E->d_absmax.as<unsigned long long>());
+    LAI_CUDA_TRY(cudaGetLastError());
+  }
+  unsigned long long bits = 0;
+  LAI_CUDA_TRY(cudaMemcpyAsync(&bits, E->d_absmax.p, sizeof(bits), cudaMemcpyDeviceToHost, stream));
+  LAI_CUDA_TRY(cudaStreamSynchronize(stream));
+  std::memcpy(out, &bits, sizeof(double));
+  return LAI_OK;
+}
+
+// Builds (once per cut value) the FP64/FP32 split of every block.
+int build_split(lai_engine* E, double cut) {
+  if (E->split_cut == cut) return LAI_OK;
+  E->split_cut = -1.0;
+  for (auto& bp : E->blocks) {
+    auto& b = *bp;
+    const auto& ca = *E->classes[b.bra];
+    const auto& cb = *E->classes[b.ket];
+    const int n = ca.n();
+    std::vector<int64_t> o64(n + 1), o32(n + 1);
+    std::vector<int> qb32(n);
+    o64[0] = o32[0] = 0;
+    for (int p = 0; p < n; ++p) {
+      const int64_t cnt = b.offsets[p + 1] - b.offsets[p];
+      int lo = 0, hi = (int)cnt;  // first ket with Q_p Q_q < cut
+      while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if (ca.Q[p] * cb.Q[mid] >= cut) lo = mid + 1; else hi = mid;
+      }
+      o64[p + 1] = o64[p] + lo;
+      o32[p + 1] = o32[p] + (cnt - lo);
+      qb32[p] = lo;
+    }
+    b.total64 = o64[n];
+    b.total32 = o32[n];
+    LAI_CUDA_TRY(upload(b.d_off64, o64));
+    LAI_CUDA_TRY(upload(b.d_off32, o32));
+    LAI_CUDA_TRY(upload(b.d_qb32, qb32));
+  }
+  E->split_cut = cut;
+  return LAI_OK;
+}
+
 int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t stream,
            const lai_jk_opts& o, lai_jk_report* rep, bool timed) {
   const int nbf = (int)E->basis->nbf;
@@ -605,10 +679,25 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
   args.mode = lai::MODE_JK;
   args.prim_eps = E->prim_eps;
   int launches = 0;
-  int64_t nq = 0;
+  int64_t nq = 0, nq32 = 0;
   double flops = 0;
+  // Mixed precision: a quartet runs in FP32 when Q_ij Q_kl max|D| < fp32_cut.  The
+  // Schwarz cut fp32_cut / max|D| is rounded down to a power of two (conservative:
+  // fewer FP32 quartets), so that the split, built on the host, is rebuilt only
+  // when max|D| moves past a power of two.
+  double cut = 0.0;
+  if (o.fp32_cut > 0.0) {
+    double maxd = 0.0;
+    if (int rc = device_absmax(E, dD, (size_t)nbf * nbf, stream, &maxd)) { E->stream = saved; return rc; }
+    if (maxd > 0.0 && std::isfinite(maxd)) cut = std::exp2(std::floor(std::log2(o.fp32_cut / maxd)));
+  }
+  const bool mixed = cut > 0.0;
+  if (mixed) {
+    if (int rc = build_split(E, cut)) { E->stream = saved; return rc; }
+  }
+  const int nparts = mixed ? 2 : 1;
   if (o.profile) {
-    const size_t need = 2 * E->blocks.size();
+    const size_t need = 2 * nparts * E->blocks.size();
     while (E->prof_ev.size() < need) {
       cudaEvent_t ev;
       LAI_CUDA_TRY(cudaEventCreate(&ev));
@@ -616,32 +705,45 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
     }
     E->prof_block.clear();
     E->prof_quartets.clear();
-    if (E->d_prof_prims.bytes < sizeof(unsigned long long) * E->blocks.size())
-      LAI_CUDA_TRY(E->d_prof_prims.alloc(sizeof(unsigned long long) * std::max<size_t>(1, E->blocks.size())));
+    if (E->d_prof_prims.bytes < sizeof(unsigned long long) * nparts * E->blocks.size())
+      LAI_CUDA_TRY(E->d_prof_prims.alloc(sizeof(unsigned long long) *
+                                         std::max<size_t>(1, nparts * E->blocks.size())));
     LAI_CUDA_TRY(cudaMemsetAsync(E->d_prof_prims.p, 0, E->d_prof_prims.bytes, stream));
   }
   E->prof_n = 0;
   for (size_t b = 0; b < E->blocks.size(); ++b) {
     const auto& bp = *E->blocks[b];
-    lai::QuartetBlock q = make_block(E, bp);
-    // this shard's contiguous slice of the block
-    const int64_t lo = bp.total * o.shard_index / o.shard_count;
-    const int64_t hi = bp.total * (o.shard_index + 1) / o.shard_count;
-    if (hi <= lo) continue;
-    q.t_begin = lo;
-    q.total = hi;
-    args.prim_count = o.profile ? E->d_prof_prims.as<unsigned long long>() + E->prof_n : nullptr;
-    if (o.profile) LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n], stream));
-    if (int rc = launch_block(E, q, args)) { E->stream = saved; return rc; }
-    if (o.profile) {
-      LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n + 1], stream));
-      E->prof_block.push_back((int)b);
-      E->prof_quartets.push_back(hi - lo);
-      ++E->prof_n;
+    for (int part = 0; part < nparts; ++part) {
+      // part 0: the whole block (FP64), or its FP64 prefix when mixed; part 1: the
+      // FP32 suffix
+      lai::QuartetBlock q = make_block(E, bp);
+      int64_t total = bp.total;
+      if (mixed) {
+        total = part == 0 ? bp.total64 : bp.total32;
+        q.offsets = (part == 0 ? bp.d_off64 : bp.d_off32).as<int64_t>();
+        q.qbegin = part == 0 ? nullptr : bp.d_qb32.as<int>();
+      }
+      // this shard's contiguous slice of the part
+      const int64_t lo = total * o.shard_index / o.shard_count;
+      const int64_t hi = total * (o.shard_index + 1) / o.shard_count;
+      if (hi <= lo) continue;
+      q.t_begin = lo;
+      q.total = hi;
+      args.prim_count = o.profile ? E->d_prof_prims.as<unsigned long long>() + E->prof_n : nullptr;
+      if (o.profile) LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n], stream));
+      bool ran32 = false;
+      if (int rc = launch_block(E, q, args, part == 1, &ran32)) { E->stream = saved; return rc; }
+      if (o.profile) {
+        LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n + 1], stream));
+        E->prof_block.push_back((int)b);
+        E->prof_quartets.push_back(hi - lo);
+        ++E->prof_n;
+      }
+      ++launches;
+      nq += hi - lo;
+      if (ran32) nq32 += hi - lo;
+      flops += bp.alg_flops * (double)(hi - lo);
     }
-    ++launches;
-    nq += hi - lo;
-    flops += bp.alg_flops * (double)(hi - lo);
   }
   const int64_t nn = (int64_t)nbf * nbf;
   if (nn > 0) {
@@ -653,8 +755,9 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
   if (timed) LAI_CUDA_TRY(cudaEventRecord(E->ev1, stream));
   E->stream = saved;
   if (rep) {
-    rep->quartets_fp64 = nq;
-    rep->quartets_fp32 = 0;
+    rep->quartets_fp64 = nq - nq32;
+    rep->quartets_fp32 = nq32;
+    rep->fp32_schwarz_cut = cut;
     rep->alg_flops = flops;
     rep->kernel_launches = launches;
     rep->seconds_device = 0;
@@ -768,7 +871,7 @@ int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d_J, doub
   lai_jk_opts o;
   lai_jk_opts_default(&o);
   if (opts) o = *opts;
-  if (o.fp32_cut != 0.0) return fail(LAI_ENOTSUP, "mixed precision not enabled in this build");
+  if (!(o.fp32_cut >= 0.0)) return fail(LAI_EINVAL, "lai_jk_build_device: fp32_cut must be >= 0");
   LAI_CUDA_TRY(cudaSetDevice(engine->device));
   return run_jk(engine, d_D, d_J, d_K, (cudaStream_t)stream, o, report, false);
 }
@@ -784,7 +887,7 @@ int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double* J, dou
   lai_jk_opts o;
   lai_jk_opts_default(&o);
   if (opts) o = *opts;
-  if (o.fp32_cut != 0.0) return fail(LAI_ENOTSUP, "mixed precision not enabled in this build");
+  if (!(o.fp32_cut >= 0.0)) return fail(LAI_EINVAL, "lai_jk_build: fp32_cut must be >= 0");
   if (o.check_symmetric) {
     for (size_t i = 0; i < nbf; ++i)
       for (size_t j = 0; j < i; ++j)

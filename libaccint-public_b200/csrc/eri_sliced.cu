@@ -44,7 +44,7 @@ __host__ __device__ constexpr int next_pow2(int x) {
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JKArgs& args,
                                                const RysTablesView& tab,
-                                               const double* __restrict__ stab, int64_t t, int p,
+                                               const R* __restrict__ stab, int64_t t, int p,
                                                bool active, int a) {
   constexpr int LAB = LA + LB, LCD = LC + LD;
   constexpr int NR = (LAB + LCD) / 2 + 1;
@@ -77,7 +77,8 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
     if (qab * blk.ket.qprim_max < peps) break;
     const R zeta = R(__ldg(pb + PF_ZETA * sb));
     const R hz = R(__ldg(pb + PF_HZ * sb));
-    const R Px = R(__ldg(pb + PF_PX * sb)), Py = R(__ldg(pb + PF_PY * sb)), Pz = R(__ldg(pb + PF_PZ * sb));
+    // P - Q in FP64 on both paths (centres are O(10) bohr)
+    const double Px = __ldg(pb + PF_PX * sb), Py = __ldg(pb + PF_PY * sb), Pz = __ldg(pb + PF_PZ * sb);
     const R PAx = R(__ldg(pb + PF_PAX * sb)), PAy = R(__ldg(pb + PF_PAY * sb)),
             PAz = R(__ldg(pb + PF_PAZ * sb));
     const R cab = R(__ldg(pb + PF_C * sb));
@@ -91,13 +92,13 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
       ++nprim_done;
       const R eta = R(cur.eta);
       const R he = R(cur.he);
-      const R PQx = Px - R(cur.px);
-      const R PQy = Py - R(cur.py);
-      const R PQz = Pz - R(cur.pz);
+      const R PQx = R(Px - cur.px);
+      const R PQy = R(Py - cur.py);
+      const R PQz = R(Pz - cur.pz);
       const R QCx = R(cur.qcx), QCy = R(cur.qcy), QCz = R(cur.qcz);
       const R ccd = R(cur.c);
       const R s = zeta + eta;
-      const R rs = R(1) / sqrt(s);
+      const R rs = fast_rsqrt(s);
       const R inv = rs * rs;
       const R rz = eta * inv, re = zeta * inv;
       const R T = zeta * rz * (PQx * PQx + PQy * PQy + PQz * PQz);
@@ -376,8 +377,9 @@ __global__ void __launch_bounds__(128) eri_sliced_kernel(QuartetBlock blk, JKArg
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   constexpr int TW = next_pow2(ncart(LA));
   constexpr int QPW = 32 / TW;  // quartets per warp
-  extern __shared__ double stab[];
-  stage_table<NR>(stab, tab);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* stab = reinterpret_cast<R*>(smem_raw);
+  stage_table<NR, R>(stab, tab);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int slot = lane / TW, a = lane % TW;
@@ -414,7 +416,7 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   constexpr int QPW = 32 / next_pow2(ncart(LA));
   const int threads = 128;
-  const size_t smem = sizeof(double) * table_doubles<NR>();
+  const size_t smem = fp32 ? table_bytes<NR, float>() : table_bytes<NR, double>();
   const int64_t nchunks = (blk.total - blk.t_begin + QPW - 1) / QPW;
   if (nchunks <= 0) return 1;
   auto kern = fp32 ? eri_sliced_kernel<LA, LB, LC, LD, float> : eri_sliced_kernel<LA, LB, LC, LD, double>;

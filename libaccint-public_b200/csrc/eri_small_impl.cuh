@@ -50,7 +50,7 @@ __device__ __forceinline__ T warp_sum(T v) {
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>
 __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKArgs& args,
                                               const RysTablesView& tab,
-                                              const double* __restrict__ stab, int64_t t, int p,
+                                              const R* __restrict__ stab, int64_t t, int p,
                                               bool active, bool uniform_bra, int ps, int sub) {
   // ps lanes (a power of two, aligned) share this quartet: lane `sub` of the group
   // runs bra primitive pairs sub, sub+ps, ...; the group then sums its partial
@@ -83,7 +83,9 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
     if (qab * blk.ket.qprim_max < peps) break;
     const R zeta = R(__ldg(pb + PF_ZETA * sb));
     const R hz = R(__ldg(pb + PF_HZ * sb));
-    const R Px = R(__ldg(pb + PF_PX * sb)), Py = R(__ldg(pb + PF_PY * sb)), Pz = R(__ldg(pb + PF_PZ * sb));
+    // P - Q is formed in FP64 on both paths: the centres are O(10) bohr, and their
+    // FP32 difference would lose the digits that T = rho |PQ|^2 needs
+    const double Px = __ldg(pb + PF_PX * sb), Py = __ldg(pb + PF_PY * sb), Pz = __ldg(pb + PF_PZ * sb);
     const R PAx = R(__ldg(pb + PF_PAX * sb)), PAy = R(__ldg(pb + PF_PAY * sb)),
             PAz = R(__ldg(pb + PF_PAZ * sb));
     const R cab = R(__ldg(pb + PF_C * sb));
@@ -97,13 +99,13 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
       ++nprim_done;
       const R eta = R(cur.eta);
       const R he = R(cur.he);
-      const R PQx = Px - R(cur.px);
-      const R PQy = Py - R(cur.py);
-      const R PQz = Pz - R(cur.pz);
+      const R PQx = R(Px - cur.px);
+      const R PQy = R(Py - cur.py);
+      const R PQz = R(Pz - cur.pz);
       const R QCx = R(cur.qcx), QCy = R(cur.qcy), QCz = R(cur.qcz);
       const R ccd = R(cur.c);
       const R s = zeta + eta;
-      const R rs = R(1) / sqrt(s);
+      const R rs = fast_rsqrt(s);
       const R inv = rs * rs;
       const R rz = eta * inv, re = zeta * inv;
       const R T = zeta * rz * (PQx * PQx + PQy * PQy + PQz * PQz);
@@ -395,8 +397,9 @@ template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>
 __global__ void __launch_bounds__(256) eri_small_kernel(QuartetBlock blk, JKArgs args,
                                                         RysTablesView tab, int kSuper, int ps) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
-  extern __shared__ double stab[];
-  stage_table<NR>(stab, tab);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* stab = reinterpret_cast<R*>(smem_raw);
+  stage_table<NR, R>(stab, tab);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   if (!SPLIT) ps = 1;
@@ -442,7 +445,7 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
                cudaStream_t stream, bool fp32, int num_sms) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   const int threads = 256;
-  const size_t smem = sizeof(double) * table_doubles<NR>();
+  const size_t smem = fp32 ? table_bytes<NR, float>() : table_bytes<NR, double>();
   const int64_t nq = blk.total - blk.t_begin;
   if (nq <= 0) return 1;
   // lanes per quartet: split the bra primitive loop when the launch has too few

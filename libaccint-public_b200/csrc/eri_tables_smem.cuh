@@ -7,33 +7,41 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "eri_device.cuh"
 #include "rys_eval.h"
 
 namespace lai {
 
-// Shared-memory table layouts (in doubles).
-constexpr int kBoysRow = 14;  // F_0..F_11 per grid point + 2 pad: 16-byte rows, stride/2 odd
+// Shared-memory table layouts, in elements of the compute type R (the FP32 kernels
+// stage FP32 copies: half the shared memory, and single-width loads).
+constexpr int kBoysRow = 14;   // FP64: F_0..F_11 per grid point + 2 pad: 16-byte rows, stride/2 odd
+constexpr int kBoysRowF = 12;  // FP32: F_0..F_11, three 16-byte units (odd)
+template <typename R>
+__host__ __device__ constexpr int boys_row() { return sizeof(R) == 8 ? kBoysRow : kBoysRowF; }
 template <int NR>
 __host__ __device__ constexpr int rys_row() { return 24 * NR + 2; }  // 12 degrees x NR x (u,w) + pad
-template <int NR>
-__host__ __device__ constexpr int table_doubles() {
-  return NR == 1 ? kBoysNGrid * kBoysRow : rys_tmax_c(NR) * rys_row<NR>();
+template <int NR, typename R>
+__host__ __device__ constexpr int table_elems() {
+  return NR == 1 ? kBoysNGrid * boys_row<R>() : rys_tmax_c(NR) * rys_row<NR>();
 }
+template <int NR, typename R>
+__host__ __device__ constexpr size_t table_bytes() { return sizeof(R) * table_elems<NR, R>(); }
 
-template <int NR>
-__device__ __forceinline__ void stage_table(double* __restrict__ st, const RysTablesView& tab) {
+template <int NR, typename R>
+__device__ __forceinline__ void stage_table(R* __restrict__ st, const RysTablesView& tab) {
   if constexpr (NR == 1) {
     for (int i = threadIdx.x; i < kBoysNGrid * 12; i += blockDim.x) {
       const int k = i / 12, j = i - k * 12;
-      st[k * kBoysRow + j] = __ldg(tab.boys + k * kBoysNM + j);
+      st[k * boys_row<R>() + j] = R(__ldg(tab.boys + k * kBoysNM + j));
     }
   } else {
     constexpr int W = 24 * NR;
     const double* src = tab.coef + rys_off(NR);
     for (int i = threadIdx.x; i < rys_tmax_c(NR) * W; i += blockDim.x) {
       const int k = i / W, j = i - k * W;
-      st[k * rys_row<NR>() + j] = __ldg(src + i);
+      st[k * rys_row<NR>() + j] = R(__ldg(src + i));
     }
   }
 }
@@ -41,62 +49,67 @@ __device__ __forceinline__ void stage_table(double* __restrict__ st, const RysTa
 // Roots/weights of the NR-point Rys rule from the staged table (same arithmetic
 // as rys_roots_table in rys_eval.h).
 template <int NR, typename R>
-__device__ __forceinline__ void rys_smem(R T, const double* __restrict__ st, const RysTablesView& tab,
+__device__ __forceinline__ void rys_smem(R T, const R* __restrict__ st, const RysTablesView& tab,
                                          R* __restrict__ u, R* __restrict__ w) {
+  constexpr bool F64 = sizeof(R) == 8;
   if constexpr (NR == 1) {
-    R F0, F1;
     if (T < R(kBoysTmax)) {
-      const int k = __double2int_rn(double(T) * 10.0);
+      // nearest grid point; in FP32, T just below kBoysTmax can round up to the
+      // row past the end, hence the clamp
+      const int k = min(F64 ? __double2int_rn(double(T) * 10.0) : __float2int_rn(float(T) * 10.0f),
+                        kBoysNGrid - 1);
       const R x = R(k) * R(0.1) - T;
-      const double2* f = reinterpret_cast<const double2*>(st + k * kBoysRow);
-      double g[12];
+      constexpr int NG = boys_terms<R>() + 1;  // grid values used: F_0..F_N
+      R g[12];
+      if constexpr (F64) {
+        const double2* f = reinterpret_cast<const double2*>(st + k * kBoysRow);
 #pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        const double2 v = f[j];
-        g[2 * j] = v.x;
-        g[2 * j + 1] = v.y;
+        for (int j = 0; j < (NG + 1) / 2; ++j) {
+          const double2 v = f[j];
+          g[2 * j] = v.x;
+          g[2 * j + 1] = v.y;
+        }
+      } else {
+        const float4* f = reinterpret_cast<const float4*>(st + k * kBoysRowF);
+#pragma unroll
+        for (int j = 0; j < (NG + 3) / 4; ++j) {
+          const float4 v = f[j];
+          g[4 * j] = v.x;
+          g[4 * j + 1] = v.y;
+          g[4 * j + 2] = v.z;
+          g[4 * j + 3] = v.w;
+        }
       }
-      R tpow[10];
-      tpow[0] = R(1);
-#pragma unroll
-      for (int j = 1; j < 10; ++j) tpow[j] = tpow[j - 1] * x * R(1.0 / j);
-      R a = 0, b = 0;
-#pragma unroll
-      for (int j = 9; j >= 0; --j) {
-        a += R(g[j]) * tpow[j];
-        b += R(g[j + 1]) * tpow[j];
-      }
-      F0 = a;
-      F1 = b;
+      R F0, F1;
+      boys_taylor<R>(x, g, F0, F1);
+      u[0] = fast_div(F1, F0);
+      w[0] = F0;
     } else {
-      const R rt = R(1) / sqrt(T);
-      F0 = R(0.88622692545275801365) * rt;
-      F1 = F0 * R(0.5) / T;
+      rys1_asymptotic<R>(T, u[0], w[0]);
     }
-    u[0] = F1 / F0;
-    w[0] = F0;
   } else {
     if (T < R(rys_tmax_c(NR))) {
       const int k = (int)T;
       const R x = R(2) * (T - R(k)) - R(1);
-      const double2* c = reinterpret_cast<const double2*>(st + k * rys_row<NR>());
+      using V2 = typename std::conditional<F64, double2, float2>::type;
+      const V2* c = reinterpret_cast<const V2*>(st + k * rys_row<NR>());
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
-        const double2 v = c[kRysDeg * NR + r];
-        u[r] = R(v.x);
-        w[r] = R(v.y);
+        const V2 v = c[kRysDeg * NR + r];
+        u[r] = v.x;
+        w[r] = v.y;
       }
 #pragma unroll
       for (int j = kRysDeg - 1; j >= 0; --j)
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-          const double2 v = c[j * NR + r];
-          u[r] = u[r] * x + R(v.x);
-          w[r] = w[r] * x + R(v.y);
+          const V2 v = c[j * NR + r];
+          u[r] = u[r] * x + v.x;
+          w[r] = w[r] * x + v.y;
         }
     } else {
-      const R it = R(1) / T;
-      const R rt = sqrt(it);
+      const R rt = fast_rsqrt(T);
+      const R it = rt * rt;
       const int h = rys_hoff(NR);
 #pragma unroll
       for (int r = 0; r < NR; ++r) {

@@ -206,3 +206,53 @@ def test_primitive_screening_is_within_tolerance(lai):
     assert r1.quartets_fp64 == r0.quartets_fp64
     assert np.max(np.abs(J1 - J0)) < 1e-11
     assert np.max(np.abs(K1 - K0)) < 1e-11
+
+
+MIXED_DE_TOL = 1e-8  # |E(mixed) - E(FP64)| bar for the FP32 Rys path (Hartree)
+
+
+def test_mixed_precision_energy_within_bar(lai):
+    """FP32 Rys path for quartets with Q_ij Q_kl max|D| < 1e-7: the energy moves by
+    less than 1e-8 Eh, J/K stay symmetric, and the FP32 path really ran (its
+    results differ from FP64 in the last digits, and the report counts it)."""
+    w = lai.workloads.make("h2o16_ccpvdz")
+    e = _engine(lai, w.basis)
+    J0, K0, r0 = e.jk(w.D)
+    J1, K1, r1 = e.jk(w.D, fp32_cut=1e-7)
+    assert r1.quartets_fp32 > 0.3 * (r1.quartets_fp32 + r1.quartets_fp64)
+    assert r1.quartets_fp32 + r1.quartets_fp64 == r0.quartets_fp64
+    maxd = np.max(np.abs(w.D))
+    assert 0.5 * 1e-7 / maxd < r1.fp32_schwarz_cut <= 1e-7 / maxd
+    E0 = lai.molecules.energy(w.D, J0, K0)
+    E1 = lai.molecules.energy(w.D, J1, K1)
+    assert abs(E1 - E0) < MIXED_DE_TOL
+    assert 0.0 < np.max(np.abs(J1 - J0)) < 1e-7
+    assert 0.0 < np.max(np.abs(K1 - K0)) < 1e-7
+    assert np.max(np.abs(J1 - J1.T)) < 1e-12 and np.max(np.abs(K1 - K1.T)) < 1e-12
+
+
+def test_mixed_precision_cut_zero_is_fp64(lai):
+    """fp32_cut = 0 is the plain FP64 build (equal up to the order of the FP64
+    atomic additions); a negative cut is an error."""
+    w = lai.workloads.make("h2o2_ccpvdz")
+    e = _engine(lai, w.basis)
+    J0, K0, _ = e.jk(w.D)
+    J1, K1, r1 = e.jk(w.D, fp32_cut=0.0)
+    assert r1.quartets_fp32 == 0 and r1.fp32_schwarz_cut == 0.0
+    assert np.max(np.abs(J0 - J1)) < 1e-13 and np.max(np.abs(K0 - K1)) < 1e-13
+    with pytest.raises(lai.LibAccIntError):
+        e.jk(w.D, fp32_cut=-1.0)
+
+
+def test_mixed_precision_all_fp32_close_to_reference(lai):
+    """Every quartet in FP32 (a cut above every bound): J/K still agree with the
+    reference's FP64 J/K to FP32 accuracy -- a check of the FP32 kernels of every
+    class present, including those that fall back to FP64 kernels."""
+    g = golden("h2o2_ccpvdz_ref.npz")
+    b = lai.BasisSet.from_atoms(g["Z"], g["xyz"], "cc-pvdz")
+    e = _engine(lai, b)
+    J, K, r = e.jk(g["D"], fp32_cut=1e30)
+    assert r.quartets_fp32 > 0.9 * (r.quartets_fp32 + r.quartets_fp64)
+    scale = max(np.max(np.abs(g["J"])), 1.0)
+    assert np.max(np.abs(J - g["J"])) < 1e-5 * scale
+    assert np.max(np.abs(K - g["K"])) < 1e-5 * scale
