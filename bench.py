@@ -289,14 +289,16 @@ def main():
     roof_all = float(np.sum(pfx) / (np.sum(pms) * 1e-3) / 1e12)
     roof_all_nominal = float(np.sum(pfl) / (np.sum(pms) * 1e-3) / 1e12)
     by_class = {}
-    for ms, fl, cl in zip(pms, pfx, pcl):
+    for ms, fl, cl, nq, npq in zip(pms, pfx, pcl, pr["quartets"], pr["prim_quartets"]):
         key = "(%s%s|%s%s)" % tuple("spdfg"[x] for x in cl)
-        a = by_class.setdefault(key, [0.0, 0.0, 0])
+        a = by_class.setdefault(key, [0.0, 0.0, 0, 0, 0])
         a[0] += ms
         a[1] += fl
         a[2] += 1
+        a[3] += int(nq)
+        a[4] += int(npq)
     # dominant kernel = the class kernel with the largest share of device time
-    dom_key, (dom_ms, dom_fl, dom_n) = max(by_class.items(), key=lambda kv: kv[1][0])
+    dom_key, (dom_ms, dom_fl, dom_n, _, _) = max(by_class.items(), key=lambda kv: kv[1][0])
     dom_tf = float(dom_fl / (dom_ms * 1e-3) / 1e12)
     traffic = TRAFFIC_PER_LAUNCH.get((args.workload, dom_key))
     prim_exec = int(np.sum(pr["prim_quartets"]))
@@ -338,7 +340,9 @@ def main():
                          "prim_quartets_executed": prim_exec,
                          "peak_source": "measured in-run: register-resident FP64 FMA loop "
                                         "(MEASURED_PEAKS.json has no FP64 entry)"},
-            "class_ms_tflops": {k: [round(v[0], 2), round(v[1] / (v[0] * 1e-3) / 1e12, 2)] for k, v in top_cls},
+            "classes": {"columns": ["ms", "TFLOP/s executed", "quartets", "primitive quartets executed"],
+                        **{k: [round(v[0], 2), round(v[1] / (v[0] * 1e-3) / 1e12, 2), v[3], v[4]]
+                           for k, v in top_cls}},
             "clocks": clk,
             "gpu_launches": launches,
             "setup_s": setup_s,

@@ -181,6 +181,76 @@ LAI_API int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_c
                                    int64_t* n_quartets, int64_t* n_values);
 
 /* ---------------------------------------------------------------------------
+ * Work units: a caller-supplied list of shell quartets, quartets[4t..4t+3] =
+ * shell indices (i, j, k, l) of quartet t, in any order and orientation.
+ * Replaces CudaEngine/CpuEngine::compute_shell_set_quartet(op, quartet, consumer,
+ * canonical_symmetry) (include/libaccint/engine/cuda_engine.hpp:462-466,792-980;
+ * include/libaccint/engine/cpu_engine.hpp:436-549) and Engine::compute_batch
+ * (include/libaccint/engine/engine.hpp:1008-1122).  No Schwarz or primitive
+ * screening is applied to a listed quartet.
+ * ------------------------------------------------------------------------- */
+/* Raw norm-corrected Cartesian integrals of each listed quartet, block t =
+ * [i][j][k][l] in the listed shell order at out + meta[t].offset (meta also gives
+ * the first functions and sizes).  out_capacity in doubles. */
+LAI_API int lai_eri_quartets(lai_engine* engine, const int32_t* quartets, int64_t n, double* out,
+                             size_t out_capacity, lai_quartet_meta* meta);
+/* J/K contributions ADDED to J and K (nbf x nbf).  canonical_symmetry = 0: plain
+ * accumulation of exactly the listed ordered quartets, J_ij += (ij|kl) D_kl,
+ * K_ik += (ij|kl) D_jl (FockBuilder::accumulate, src/shared/consumers/fock_builder.cpp:64-121);
+ * = 1: each listed quartet stands for its whole 8-fold permutation orbit, with the
+ * degeneracy of equal shells (accumulate_symmetric, fock_builder.cpp:123-222).
+ * Host buffers; the device variant takes device D/J/K and returns after the
+ * kernels finished (the per-call pair tables are freed on return). */
+LAI_API int lai_jk_accumulate_quartets(lai_engine* engine, const int32_t* quartets, int64_t n,
+                                       const double* D, double* J, double* K, int canonical_symmetry);
+LAI_API int lai_jk_accumulate_quartets_device(lai_engine* engine, const int32_t* quartets, int64_t n,
+                                              const double* d_D, double* d_J, double* d_K, void* stream,
+                                              int canonical_symmetry);
+/* Plain J/K accumulation of an integral batch already on the device: block t is
+ * d_eri[meta[t].offset ...], [a][b][c][d] over functions fa.., sizes na.. (meta on
+ * the host).  Replaces GpuFockBuilder::accumulate_device_eri_batch
+ * (src/device/cuda/consumers/fock_builder_gpu.cu:600-621). */
+LAI_API int lai_jk_accumulate_eri_batch_device(lai_engine* engine, const double* d_eri,
+                                               const lai_quartet_meta* meta, int64_t n, const double* d_D,
+                                               double* d_J, double* d_K, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Nuclear gradient of E = 1/2 tr(D J[D]) - 1/4 tr(D K[D]) at fixed D, over the
+ * engine's screened canonical quartets (those the J/K build computes):
+ * dE/dR_A = sum_q s_q sum_abcd d(ab|cd)/dR_A (4 D_ab D_cd - D_ac D_bd - D_ad D_bc),
+ * with derivative integrals formed and contracted on the fly.  dE/dD = J - K/2
+ * comes from the J/K build.  No counterpart in the reference, which has no
+ * derivative integrals (config.hpp.in:49, MAX_DERIVATIVE_ORDER = 0).  Needs the
+ * basis created with atom indices; grad is [natom][3] (Hartree/Bohr), natom =
+ * 1 + the largest atom index (lai_engine_natom).
+ * ------------------------------------------------------------------------- */
+LAI_API int lai_engine_natom(lai_engine* engine);
+LAI_API int lai_jk_gradient(lai_engine* engine, const double* D, size_t nbf, double* grad);
+/* Device D and grad; asynchronous on stream. */
+LAI_API int lai_jk_gradient_device(lai_engine* engine, const double* d_D, double* d_grad, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Cartesian -> spherical (real solid harmonics, l <= 4).  The J/K path is
+ * Cartesian, as in the reference; these move D in and J/K out of a spherical
+ * basis: D_cart = T^T D_sph T, M_sph = T M_cart T^T, T = block-diag(C_l).
+ * Replaces math::get_cart_to_sph_matrix / transform_2d
+ * (include/libaccint/math/spherical_transform.hpp:20-70): same orders
+ * (spherical m = 0, 1, -1, 2, -2, ...; Cartesian lx, then ly descending).
+ * ------------------------------------------------------------------------- */
+/* C_l, (2l+1) x (l+1)(l+2)/2 row-major. */
+LAI_API int lai_cart_to_sph_matrix(int l, double* C);
+/* Number of spherical functions of the basis (sum of 2l+1), or -1. */
+LAI_API long lai_basis_nbf_spherical(const lai_basis* basis);
+/* Host: M_sph (nsph x nsph) = T M_cart T^T;  D_cart (ncart x ncart) = T^T D_sph T. */
+LAI_API int lai_cart_to_sph_2d(const lai_basis* basis, const double* M_cart, double* M_sph);
+LAI_API int lai_sph_to_cart_density(const lai_basis* basis, const double* D_sph, double* D_cart);
+/* The same on the engine's device (device pointers; asynchronous on stream). */
+LAI_API int lai_cart_to_sph_2d_device(lai_engine* engine, const double* d_M_cart, double* d_M_sph,
+                                      void* stream);
+LAI_API int lai_sph_to_cart_density_device(lai_engine* engine, const double* d_D_sph, double* d_D_cart,
+                                           void* stream);
+
+/* ---------------------------------------------------------------------------
  * Measurement helpers (no counterpart in the reference, which has no device
  * profiling of this path).
  * ------------------------------------------------------------------------- */

@@ -4,6 +4,6 @@ Import with ``importlib.import_module("libaccint-public_b200")`` (the package
 directory name is not a Python identifier).
 """
 from ._lib import LibAccIntError, lib  # noqa: F401
-from .basis import BasisSet, Shell, basis_data  # noqa: F401
+from .basis import BasisSet, Shell, basis_data, cart_to_sph_matrix  # noqa: F401
 from .engine import Engine, FockBuilder, Operator, ScreeningOptions, jk, probe_fp64_peak  # noqa: F401
-from . import molecules, workloads  # noqa: F401
+from . import autograd, molecules, workloads  # noqa: F401

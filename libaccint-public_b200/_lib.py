@@ -21,6 +21,11 @@ EXPORTED = [
     "lai_jk_opts_default", "lai_jk_build", "lai_jk_build_device", "lai_eri_batch_screened",
     "lai_jk_last_profile", "lai_engine_sample_quartets", "lai_engine_quartet_count",
     "lai_probe_fp64_peak", "lai_jk_build_noalloc",
+    "lai_cart_to_sph_matrix", "lai_basis_nbf_spherical", "lai_cart_to_sph_2d", "lai_sph_to_cart_density",
+    "lai_cart_to_sph_2d_device", "lai_sph_to_cart_density_device",
+    "lai_eri_quartets", "lai_jk_accumulate_quartets", "lai_jk_accumulate_quartets_device",
+    "lai_jk_accumulate_eri_batch_device",
+    "lai_engine_natom", "lai_jk_gradient", "lai_jk_gradient_device",
 ]
 
 
@@ -87,6 +92,19 @@ def lib():
         "lai_engine_quartet_count": (ctypes.c_int64, [P]),
         "lai_probe_fp64_peak": (I, [I, ctypes.POINTER(ctypes.c_double)]),
         "lai_jk_build_noalloc": (I, [P, P, P, P, P]),
+        "lai_cart_to_sph_matrix": (I, [I, P]),
+        "lai_basis_nbf_spherical": (L64, [P]),
+        "lai_cart_to_sph_2d": (I, [P, P, P]),
+        "lai_sph_to_cart_density": (I, [P, P, P]),
+        "lai_cart_to_sph_2d_device": (I, [P, P, P, P]),
+        "lai_sph_to_cart_density_device": (I, [P, P, P, P]),
+        "lai_eri_quartets": (I, [P, P, ctypes.c_int64, P, ctypes.c_size_t, P]),
+        "lai_jk_accumulate_quartets": (I, [P, P, ctypes.c_int64, P, P, P, I]),
+        "lai_jk_accumulate_quartets_device": (I, [P, P, ctypes.c_int64, P, P, P, P, I]),
+        "lai_jk_accumulate_eri_batch_device": (I, [P, P, P, ctypes.c_int64, P, P, P, P]),
+        "lai_engine_natom": (I, [P]),
+        "lai_jk_gradient": (I, [P, P, ctypes.c_size_t, P]),
+        "lai_jk_gradient_device": (I, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -33,6 +33,14 @@ def basis_data(name):
     return _cache[key]
 
 
+def cart_to_sph_matrix(l):
+    """C_l [(2l+1) x (l+1)(l+2)/2] of real solid harmonics (spherical m = 0, 1, -1,
+    ...; Cartesian lx, then ly descending) -- get_cart_to_sph_matrix of the reference."""
+    C = np.zeros((2 * l + 1, (l + 1) * (l + 2) // 2))
+    _lib.check(_lib.lib().lai_cart_to_sph_matrix(int(l), C.ctypes.data))
+    return C
+
+
 class Shell:
     __slots__ = ("l", "center", "exps", "coefs", "atom")
 
@@ -110,6 +118,30 @@ class BasisSet:
                                           ctypes.byref(h)))
             self._handle = h
         return self._handle
+
+    @property
+    def nbf_spherical(self):
+        return sum(2 * s.l + 1 for s in self.shells)
+
+    def cart_to_sph(self, M_cart):
+        """T M_cart T^T: a Cartesian two-index matrix (J, K, F) in the spherical basis."""
+        n, ns = self.nbf, self.nbf_spherical
+        M = np.ascontiguousarray(M_cart, dtype=np.float64)
+        if M.shape != (n, n):
+            raise ValueError(f"matrix must be {n}x{n}")
+        out = np.empty((ns, ns))
+        _lib.check(_lib.lib().lai_cart_to_sph_2d(self.handle(), M.ctypes.data, out.ctypes.data))
+        return out
+
+    def sph_to_cart_density(self, D_sph):
+        """T^T D_sph T: a spherical density on the Cartesian functions the J/K path uses."""
+        n, ns = self.nbf, self.nbf_spherical
+        D = np.ascontiguousarray(D_sph, dtype=np.float64)
+        if D.shape != (ns, ns):
+            raise ValueError(f"density must be {ns}x{ns}")
+        out = np.empty((n, n))
+        _lib.check(_lib.lib().lai_sph_to_cart_density(self.handle(), D.ctypes.data, out.ctypes.data))
+        return out
 
     def normalized_coefs(self):
         """Normalized coefficients per shell as computed by the library."""

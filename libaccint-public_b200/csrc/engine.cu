@@ -30,14 +30,22 @@
 #include <vector>
 
 #include "../../include/libaccint_b200.h"
+#include "engine_internal.h"
 #include "eri_kernels.h"
 #include "rys_tables.inc"
+
+namespace lai {
+void spherical_forget_basis(const lai_basis* basis);  // spherical.cu
+}  // namespace lai
+
+using namespace lai::host;
 
 static_assert(RYS_DEG == lai::kRysDeg, "table degree mismatch");
 static_assert(BOYS_NM == lai::kBoysNM, "Boys table width mismatch");
 static_assert(BOYS_NGRID == lai::kBoysNGrid, "Boys grid mismatch");
 
-namespace {
+namespace lai {
+namespace host {
 
 thread_local std::string g_last_error;
 
@@ -46,61 +54,18 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-#define LAI_CUDA_TRY(expr)                                                              \
-  do {                                                                                  \
-    cudaError_t e_ = (expr);                                                            \
-    if (e_ != cudaSuccess)                                                              \
-      return fail(e_ == cudaErrorMemoryAllocation ? LAI_ENOMEM : LAI_ECUDA,             \
-                  std::string(#expr) + ": " + cudaGetErrorString(e_));                  \
-  } while (0)
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() { if (p) cudaFree(p); }
-  cudaError_t alloc(size_t n) {
-    if (p) { cudaFree(p); p = nullptr; }
-    bytes = n;
-    if (n == 0) return cudaSuccess;
-    return cudaMalloc(&p, n);
-  }
-  template <typename T> T* as() const { return static_cast<T*>(p); }
-};
-
-template <typename T>
-cudaError_t upload(DevBuf& b, const std::vector<T>& v) {
-  cudaError_t e = b.alloc(v.size() * sizeof(T));
-  if (e != cudaSuccess || v.empty()) return e;
-  return cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
-}
-
 double dfact_odd(int l) {
   double r = 1;
   for (int k = 2 * l - 1; k > 1; k -= 2) r *= k;
   return r;
 }
 
-}  // namespace
+}  // namespace host
+}  // namespace lai
 
 // ---------------------------------------------------------------------------
 // Basis
 // ---------------------------------------------------------------------------
-struct HostShell {
-  int l;
-  double center[3];
-  std::vector<double> exps_all, coefs_all;  // normalized, all primitives as given
-  std::vector<double> exps, coefs;          // nonzero-coefficient primitives only
-  int atom;
-  long func;
-};
-
-struct lai_basis {
-  std::vector<HostShell> shells;
-  long nbf = 0;
-};
 
 extern "C" {
 
@@ -166,7 +131,11 @@ int lai_basis_create(int nshell, const int* l, const int* nprim, const double* c
   return LAI_OK;
 }
 
-void lai_basis_destroy(lai_basis* basis) { delete basis; }
+void lai_basis_destroy(lai_basis* basis) {
+  if (!basis) return;
+  lai::spherical_forget_basis(basis);
+  delete basis;
+}
 long lai_basis_nbf(const lai_basis* basis) { return basis ? basis->nbf : 0; }
 int lai_basis_nshell(const lai_basis* basis) { return basis ? (int)basis->shells.size() : 0; }
 
@@ -189,44 +158,9 @@ int lai_basis_shell(const lai_basis* basis, int s, int* l, int* nprim, double* c
 // ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
-namespace {
+namespace lai {
+namespace host {
 
-struct PairClassHost {
-  int la, lb, Ka, Kb;
-  double qprim_max = 0.0;
-  std::vector<int> sa, sb, fa, fb;  // shell and function indices (oriented)
-  std::vector<double> Q;
-  std::vector<double> AB;          // SoA [3][n]
-  std::vector<double> prim;        // SoA [PF_COUNT][Kab][n]
-  int n() const { return (int)sa.size(); }
-  // device copies
-  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_prim;
-  lai::PairClassDev view() const {
-    lai::PairClassDev v;
-    v.la = la; v.lb = lb; v.Ka = Ka; v.Kb = Kb; v.npairs = n();
-    v.shell_a = d_sa.as<int>(); v.shell_b = d_sb.as<int>();
-    v.func_a = d_fa.as<int>(); v.func_b = d_fb.as<int>();
-    v.Q = d_Q.as<double>(); v.AB = d_AB.as<double>(); v.prim = d_prim.as<double>();
-    v.qprim_max = qprim_max;
-    return v;
-  }
-};
-
-struct ClassPairBlock {
-  int bra, ket;                 // class indices, bra >= ket
-  std::vector<int64_t> offsets; // host copy
-  DevBuf d_offsets;
-  int64_t total = 0;
-  double alg_flops = 0;         // per quartet of this block (all nonzero primitives)
-  double flops_per_prim = 0;    // per primitive quartet
-  double flops_per_quartet = 0; // per contracted quartet (normalization + digestion)
-  // Mixed-precision split of this block for one FP32 cut: the kets of bra pair p
-  // are sorted by Schwarz bound, so those with Q_p Q_q >= cut form a prefix (the
-  // FP64 part, offsets64) and the rest a suffix (the FP32 part: offsets32, with
-  // qbegin32[p] its first ket).
-  int64_t total64 = 0, total32 = 0;
-  DevBuf d_off64, d_off32, d_qb32;
-};
 
 // Algorithmic FP work of one canonical quartet (one unit), the single accounting
 // used for roofline fractions:  P (40 + 64 n + n (20 + T2D + 4 Ncart)) + 25 Ncart
@@ -258,44 +192,12 @@ __global__ void symmetrize_kernel(const double* __restrict__ Jp, const double* _
   K[idx] = Kp[idx] + Kp[tr];
 }
 
-}  // namespace
+}  // namespace host
+}  // namespace lai
 
-struct lai_engine {
-  const lai_basis* basis = nullptr;
-  int device = 0;
-  int num_sms = 148;
-  double thr = 1e-12;
-  double prim_eps = 1e-15;
-  cudaStream_t stream = nullptr;
-  DevBuf d_coef, d_hx2, d_hw, d_boys;
-  lai::RysTablesView tab{};
-  std::vector<std::unique_ptr<PairClassHost>> classes;
-  std::vector<std::unique_ptr<ClassPairBlock>> blocks;
-  std::vector<double> Q_all;     // nshell x nshell Schwarz matrix
-  DevBuf d_Jp, d_Kp, d_D, d_J, d_K;
-  DevBuf d_scratch;
-  size_t scratch_doubles = 0;
-  DevBuf d_status;
-  double split_cut = -1.0;       // FP32 cut the blocks' mixed-precision split was built for
-  DevBuf d_absmax;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  // per-launch profile of the last build with opts.profile
-  std::vector<cudaEvent_t> prof_ev;
-  std::vector<int> prof_block;
-  std::vector<int64_t> prof_quartets;
-  DevBuf d_prof_prims;
-  int prof_n = 0;
-  ~lai_engine() {
-    for (auto e : prof_ev) cudaEventDestroy(e);
-    classes.clear();
-    blocks.clear();
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
-    if (stream) cudaStreamDestroy(stream);
-  }
-};
 
-namespace {
+namespace lai {
+namespace host {
 
 int build_classes(lai_engine* E) {
   const auto& sh = E->basis->shells;
@@ -358,6 +260,7 @@ void fill_pair_data(const lai_basis* basis, PairClassHost& c) {
         const double z = al + be;
         auto at = [&](int f) -> double& { return c.prim[((size_t)f * Kab + t) * n + p]; };
         at(lai::PF_ZETA) = z;
+        at(lai::PF_ALPHA) = al;
         at(lai::PF_HZ) = 0.5 / z;
         for (int x = 0; x < 3; ++x) {
           const double P = (al * A.center[x] + be * B.center[x]) / z;
@@ -391,7 +294,7 @@ int ensure_scratch(lai_engine* E, size_t doubles) {
 // Launches the kernel of the block's class.  fp32 asks for the FP32 variant; the
 // classes without one (generic kernel) run in FP64, and *ran_fp32 says which ran.
 int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs& args,
-                 bool fp32 = false, bool* ran_fp32 = nullptr) {
+                 bool fp32, bool* ran_fp32) {
   const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
   if (ran_fp32) *ran_fp32 = false;
   if (lai::small_class_supported(la, lb, lc, ld)) {
@@ -788,7 +691,8 @@ __global__ void fp64_fma_probe(double* out, int iters) {
   if (r == 12345.678) out[0] = r;  // keep the chain alive
 }
 
-}  // namespace
+}  // namespace host
+}  // namespace lai
 
 extern "C" {
 
@@ -1083,6 +987,7 @@ int engine_num_sms(const lai_engine* E) { return E->num_sms; }
 int engine_nbf(const lai_engine* E) { return (int)E->basis->nbf; }
 double engine_prim_eps(const lai_engine* E) { return E->prim_eps; }
 RysTablesView engine_tables(const lai_engine* E) { return E->tab; }
+const lai_basis* engine_basis(const lai_engine* E) { return E->basis; }
 int engine_block_count(const lai_engine* E) { return (int)E->blocks.size(); }
 QuartetBlock engine_block(const lai_engine* E, int i) { return make_block(E, *E->blocks[i]); }
 void engine_set_error(const char* msg) { g_last_error = msg; }

@@ -116,6 +116,33 @@ __device__ __forceinline__ void load_ket_prim(const double* __restrict__ pk, siz
   k.c = __ldg(pk + PF_C * sk);
 }
 
+// Bra primitive-pair data of one pair (same fields, bra side).
+struct BraPrim {
+  double q, zeta, hz, px, py, pz, pax, pay, paz, c;
+};
+__device__ __forceinline__ void load_bra_prim(const double* __restrict__ pb, size_t sb, BraPrim& b) {
+  b.q = __ldg(pb + PF_Q * sb);
+  b.zeta = __ldg(pb + PF_ZETA * sb);
+  b.hz = __ldg(pb + PF_HZ * sb);
+  b.px = __ldg(pb + PF_PX * sb);
+  b.py = __ldg(pb + PF_PY * sb);
+  b.pz = __ldg(pb + PF_PZ * sb);
+  b.pax = __ldg(pb + PF_PAX * sb);
+  b.pay = __ldg(pb + PF_PAY * sb);
+  b.paz = __ldg(pb + PF_PAZ * sb);
+  b.c = __ldg(pb + PF_C * sb);
+}
+
+// Requests the cache lines of one primitive pair's fields into L1 without
+// waiting (PTX prefetch.global.L1): the loads that follow later hit L1.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+__device__ __forceinline__ void prefetch_prim_l1(const double* __restrict__ pp, size_t s) {
+#pragma unroll
+  for (int f = 0; f < PF_COUNT; ++f) prefetch_l1(pp + f * s);
+}
+
 // Add a per-lane count to a launch counter (one atomic per warp).
 __device__ __forceinline__ void count_prims(unsigned long long* ctr, unsigned int n) {
   if (!ctr) return;
@@ -139,10 +166,12 @@ __device__ __forceinline__ int find_bra(const int64_t* __restrict__ offsets, int
 // 1/2 for each of i==j, k==l, (ij)==(kl) (the permutation flags of the reference's
 // accumulate_symmetric, src/shared/consumers/fock_builder.cpp:123-222).
 __device__ __forceinline__ double quartet_weight(const QuartetBlock& blk, int p, int q) {
+  const int a = __ldg(blk.bra.shell_a + p), b = __ldg(blk.bra.shell_b + p);
+  const int c = __ldg(blk.ket.shell_a + q), d = __ldg(blk.ket.shell_b + q);
   double s = 1.0;
-  if (__ldg(blk.bra.shell_a + p) == __ldg(blk.bra.shell_b + p)) s *= 0.5;
-  if (__ldg(blk.ket.shell_a + q) == __ldg(blk.ket.shell_b + q)) s *= 0.5;
-  if (blk.same_class && p == q) s *= 0.5;
+  if (a == b) s *= 0.5;
+  if (c == d) s *= 0.5;
+  if (a == c && b == d) s *= 0.5;  // same (oriented) shell pair on both sides
   return s;
 }
 

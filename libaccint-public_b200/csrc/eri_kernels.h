@@ -26,4 +26,11 @@ int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesV
 // its (e0|f0) block does not fit in shared memory; 0 if it fits.
 size_t generic_global_scratch_doubles(int la, int lb, int lc, int ld, int num_sms);
 
+// Nuclear-gradient kernel (eri_grad.cu): adds dE/dR of the block's quartets to
+// grad[natom][3] (E = 1/2 tr DJ - 1/4 tr DK at fixed D).  0 on success.
+int launch_grad(const QuartetBlock& blk, const double* D, int nbf, const int* shell_atom, double* grad,
+                double prim_eps, const RysTablesView& tab, cudaStream_t stream, double* gscratch,
+                size_t gscratch_doubles, int num_sms);
+size_t grad_global_scratch_doubles(int la, int lb, int lc, int ld, int num_sms);
+
 }  // namespace lai

@@ -110,6 +110,28 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
       const R rz = eta * inv, re = zeta * inv;
       const R T = zeta * rz * (PQx * PQx + PQy * PQy + PQz * PQz);
       const R pref = cab * ccd * rs;
+      if constexpr (NR == 1) {
+        // One root: (ss|ss) = pref F_0 and (p_i s|ss) = pref (PA_i F_0 - rz PQ_i F_1)
+        // -- the one-point Rys rule (w = F_0, u = F_1/F_0) written without its
+        // quotient.
+        R F0, F1;
+        boys01_smem<R>(T, stab, F0, F1);
+        const R pw0 = pref * F0;
+        if constexpr (LAB == 0) {
+          G[0] += pw0;
+        } else {
+          static_assert(LA == 1 && LB == 0 && LCD == 0, "one-root classes: (ss|ss), (ps|ss)");
+          const R pw1 = pref * rz * F1;
+          const R PA[3] = {PAx, PAy, PAz}, PQ[3] = {PQx, PQy, PQz};
+          sfor<0, NE>([&](auto IE) {
+            constexpr int ie = decltype(IE)::value;
+            constexpr int ce = cart_comp(LA, ie);
+            constexpr int d = comp_x(ce) ? 0 : comp_y(ce) ? 1 : 2;
+            G[ie] += PA[d] * pw0 - PQ[d] * pw1;
+          });
+        }
+        continue;
+      }
       R u[NR], w[NR];
       rys_smem<NR, R>(T, stab, tab, u, w);
 #pragma unroll
@@ -393,9 +415,12 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   }
 }
 
+// (ss|ss) is latency bound with short dependent chains and fits 64 registers:
+// ask for 4 blocks (32 warps) per SM.  The other classes keep ptxas's own choice
+// (0 = no bound; an explicit 1 would let it take up to 255 registers).
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>
-__global__ void __launch_bounds__(256) eri_small_kernel(QuartetBlock blk, JKArgs args,
-                                                        RysTablesView tab, int kSuper, int ps) {
+__global__ void __launch_bounds__(256, (LA + LB + LC + LD == 0 ? 4 : 0))
+    eri_small_kernel(QuartetBlock blk, JKArgs args, RysTablesView tab, int kSuper, int ps) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* stab = reinterpret_cast<R*>(smem_raw);

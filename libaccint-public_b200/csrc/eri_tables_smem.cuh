@@ -16,7 +16,7 @@ namespace lai {
 
 // Shared-memory table layouts, in elements of the compute type R (the FP32 kernels
 // stage FP32 copies: half the shared memory, and single-width loads).
-constexpr int kBoysRow = 14;   // FP64: F_0..F_11 per grid point + 2 pad: 16-byte rows, stride/2 odd
+constexpr int kBoysRow = 10;   // FP64: F_0..F_9 per grid point, five 16-byte units (odd)
 constexpr int kBoysRowF = 12;  // FP32: F_0..F_11, three 16-byte units (odd)
 template <typename R>
 __host__ __device__ constexpr int boys_row() { return sizeof(R) == 8 ? kBoysRow : kBoysRowF; }
@@ -27,14 +27,17 @@ __host__ __device__ constexpr int table_elems() {
   return NR == 1 ? kBoysNGrid * boys_row<R>() : rys_tmax_c(NR) * rys_row<NR>();
 }
 template <int NR, typename R>
-__host__ __device__ constexpr size_t table_bytes() { return sizeof(R) * table_elems<NR, R>(); }
+__host__ __device__ constexpr size_t table_bytes() {
+  return (sizeof(R) * table_elems<NR, R>() + 15) & ~size_t(15);  // what follows stays 16-byte aligned
+}
 
 template <int NR, typename R>
 __device__ __forceinline__ void stage_table(R* __restrict__ st, const RysTablesView& tab) {
   if constexpr (NR == 1) {
-    for (int i = threadIdx.x; i < kBoysNGrid * 12; i += blockDim.x) {
-      const int k = i / 12, j = i - k * 12;
-      st[k * boys_row<R>() + j] = R(__ldg(tab.boys + k * kBoysNM + j));
+    constexpr int NV = boys_row<R>();  // values per row (the row holds no padding)
+    for (int i = threadIdx.x; i < kBoysNGrid * NV; i += blockDim.x) {
+      const int k = i / NV, j = i - k * NV;
+      st[k * NV + j] = R(__ldg(tab.boys + k * kBoysNM + j));
     }
   } else {
     constexpr int W = 24 * NR;
@@ -46,6 +49,46 @@ __device__ __forceinline__ void stage_table(R* __restrict__ st, const RysTablesV
   }
 }
 
+// F_0(T) and F_1(T) from the staged Boys grid (same arithmetic as boys01 in
+// rys_eval.h).
+template <typename R>
+__device__ __forceinline__ void boys01_smem(R T, const R* __restrict__ st, R& F0, R& F1) {
+  constexpr bool F64 = sizeof(R) == 8;
+  if (T < R(kBoysTmax)) {
+    // nearest grid point; in FP32, T just below kBoysTmax can round up to the
+    // row past the end, hence the clamp
+    const int k = min(F64 ? __double2int_rn(double(T) * 10.0) : __float2int_rn(float(T) * 10.0f),
+                      kBoysNGrid - 1);
+    const R x = R(k) * R(0.1) - T;
+    constexpr int NG = boys_terms<R>() + 1;  // grid values used: F_0..F_N
+    R g[12];
+    if constexpr (F64) {
+      const double2* f = reinterpret_cast<const double2*>(st + k * kBoysRow);
+#pragma unroll
+      for (int j = 0; j < (NG + 1) / 2; ++j) {
+        const double2 v = f[j];
+        g[2 * j] = v.x;
+        g[2 * j + 1] = v.y;
+      }
+    } else {
+      const float4* f = reinterpret_cast<const float4*>(st + k * kBoysRowF);
+#pragma unroll
+      for (int j = 0; j < (NG + 3) / 4; ++j) {
+        const float4 v = f[j];
+        g[4 * j] = v.x;
+        g[4 * j + 1] = v.y;
+        g[4 * j + 2] = v.z;
+        g[4 * j + 3] = v.w;
+      }
+    }
+    boys_taylor<R>(x, g, F0, F1);
+  } else {
+    const R rt = fast_rsqrt(T);
+    F0 = R(0.88622692545275801365) * rt;  // sqrt(pi)/2
+    F1 = R(0.5) * F0 * rt * rt;
+  }
+}
+
 // Roots/weights of the NR-point Rys rule from the staged table (same arithmetic
 // as rys_roots_table in rys_eval.h).
 template <int NR, typename R>
@@ -54,34 +97,8 @@ __device__ __forceinline__ void rys_smem(R T, const R* __restrict__ st, const Ry
   constexpr bool F64 = sizeof(R) == 8;
   if constexpr (NR == 1) {
     if (T < R(kBoysTmax)) {
-      // nearest grid point; in FP32, T just below kBoysTmax can round up to the
-      // row past the end, hence the clamp
-      const int k = min(F64 ? __double2int_rn(double(T) * 10.0) : __float2int_rn(float(T) * 10.0f),
-                        kBoysNGrid - 1);
-      const R x = R(k) * R(0.1) - T;
-      constexpr int NG = boys_terms<R>() + 1;  // grid values used: F_0..F_N
-      R g[12];
-      if constexpr (F64) {
-        const double2* f = reinterpret_cast<const double2*>(st + k * kBoysRow);
-#pragma unroll
-        for (int j = 0; j < (NG + 1) / 2; ++j) {
-          const double2 v = f[j];
-          g[2 * j] = v.x;
-          g[2 * j + 1] = v.y;
-        }
-      } else {
-        const float4* f = reinterpret_cast<const float4*>(st + k * kBoysRowF);
-#pragma unroll
-        for (int j = 0; j < (NG + 3) / 4; ++j) {
-          const float4 v = f[j];
-          g[4 * j] = v.x;
-          g[4 * j + 1] = v.y;
-          g[4 * j + 2] = v.z;
-          g[4 * j + 3] = v.w;
-        }
-      }
       R F0, F1;
-      boys_taylor<R>(x, g, F0, F1);
+      boys01_smem<R>(T, st, F0, F1);
       u[0] = fast_div(F1, F0);
       w[0] = F0;
     } else {

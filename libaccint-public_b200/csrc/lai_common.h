@@ -37,6 +37,7 @@ enum PrimField : int {
   PF_C,          // sqrt(2) pi^{5/4} c_a c_b exp(-alpha_a alpha_b |AB|^2 / zeta) / zeta
   PF_Q,          // primitive Schwarz bound sqrt(max |(a_p b_q|a_p b_q)|); primitive pairs
                  // of each shell pair are stored in descending PF_Q order
+  PF_ALPHA,      // alpha_a, the exponent on the first shell (nuclear derivatives)
   PF_COUNT
 };
 

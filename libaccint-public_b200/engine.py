@@ -138,6 +138,13 @@ class Engine:
                                   ctypes.byref(opts), ctypes.byref(rep)))
         return J, K, rep
 
+    def jk_spherical(self, D_sph, fp32_cut=0.0):
+        """(J_sph, K_sph, report) for a density in the spherical basis: the Cartesian
+        build on T^T D_sph T, then T J T^T and T K T^T."""
+        Dc = self.basis.sph_to_cart_density(D_sph)
+        J, K, rep = self.jk(Dc, fp32_cut=fp32_cut)
+        return self.basis.cart_to_sph(J), self.basis.cart_to_sph(K), rep
+
     def jk_device(self, d_D, d_J, d_K, stream=0, fp32_cut=0.0, shard=(0, 1), profile=False):
         """Device-pointer variant (integers from torch.Tensor.data_ptr())."""
         L = _lib.lib()
@@ -187,6 +194,53 @@ class Engine:
         m = np.array([(x.offset, x.fa, x.fb, x.fc, x.fd, x.na, x.nb, x.nc, x.nd)
                       for x in meta[:nq.value]], dtype=np.int64).reshape(-1, 9)
         return out[:nv.value], m
+
+    def eri_quartets(self, quartets):
+        """Raw integrals of listed shell quartets ([n][4] shell indices, any order):
+        (values, meta) as compute_batch_screened, block t = [i][j][k][l]."""
+        L = _lib.lib()
+        q = np.ascontiguousarray(quartets, dtype=np.int32).reshape(-1, 4)
+        n = len(q)
+        if n and (q.min() < 0 or q.max() >= self.basis.n_shells):
+            raise _lib.LibAccIntError(_lib.LAI_EINVAL, "quartet list: shell index out of range")
+        nc = np.array([(s.l + 1) * (s.l + 2) // 2 for s in self.basis.shells])
+        nv = int(np.sum(nc[q[:, 0]] * nc[q[:, 1]] * nc[q[:, 2]] * nc[q[:, 3]])) if n else 0
+        out = np.zeros(max(nv, 1))
+        meta = (_lib.QuartetMeta * max(n, 1))()
+        _lib.check(L.lai_eri_quartets(self._h, q.ctypes.data, n, out.ctypes.data, out.size, meta))
+        m = np.array([(x.offset, x.fa, x.fb, x.fc, x.fd, x.na, x.nb, x.nc, x.nd)
+                      for x in meta[:n]], dtype=np.int64).reshape(-1, 9)
+        return out[:nv], m
+
+    def jk_accumulate_quartets(self, quartets, D, J, K, canonical_symmetry=True):
+        """Adds the J/K contributions of listed quartets to J and K (host arrays,
+        modified in place): plain accumulation of exactly those ordered quartets, or
+        with canonical_symmetry each standing for its 8-fold orbit."""
+        q = np.ascontiguousarray(quartets, dtype=np.int32).reshape(-1, 4)
+        n = self.basis.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        for M in (D, J, K):
+            if M.shape != (n, n) or (M is not D and not M.flags.c_contiguous):
+                raise ValueError(f"D, J, K must be contiguous {n}x{n} arrays")
+        _lib.check(_lib.lib().lai_jk_accumulate_quartets(self._h, q.ctypes.data, len(q), D.ctypes.data,
+                                                         J.ctypes.data, K.ctypes.data,
+                                                         int(bool(canonical_symmetry))))
+
+    def natom(self):
+        n = _lib.lib().lai_engine_natom(self._h)
+        if n < 0:
+            _lib.check(n)
+        return n
+
+    def gradient(self, D):
+        """dE/dR [natom][3] of E = 1/2 tr(DJ) - 1/4 tr(DK) at fixed D."""
+        n = self.basis.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        if D.shape != (n, n):
+            raise ValueError(f"density must be {n}x{n}")
+        g = np.zeros((self.natom(), 3))
+        _lib.check(_lib.lib().lai_jk_gradient(self._h, D.ctypes.data, n, g.ctypes.data))
+        return g
 
     def compute_and_consume(self, op, consumer, screening=None):
         if not op.is_two_electron():

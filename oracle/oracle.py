@@ -42,6 +42,7 @@ def restatement():
         L.orc_normalize.argtypes = [_I, _I, _P, _P, _P]
         L.orc_eri_quartet.argtypes = [_P, _P, _P, _P, _P, _P]
         L.orc_basis_quartet.argtypes = [_I, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P]
+        L.orc_basis_quartets.argtypes = [_I, _P, _P, _P, _P, _P, _L, _P, _P]
         L.orc_schwarz.argtypes = [_I, _P, _P, _P, _P, _P, _P]
         L.orc_jk_sym.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _D]
         L.orc_jk_sym.restype = ctypes.c_long
@@ -79,8 +80,19 @@ def reference():
         L.ref_time_quartets.restype = _D
         L.ref_time_quartets.argtypes = [_P, _P, _P, _L, _I, _P, _P]
         L.ref_max_threads.restype = _I
+        L.ref_cart_to_sph.restype = _I
+        L.ref_cart_to_sph.argtypes = [_I, _P]
         _ref = L
     return _ref
+
+
+def ref_cart_to_sph(l):
+    """The reference's math::get_cart_to_sph_matrix(l) (spherical_transform.hpp:20-40)."""
+    R = reference()
+    C = np.zeros((2 * l + 1, (l + 1) * (l + 2) // 2))
+    if R.ref_cart_to_sph(l, C.ctypes.data) < 0:
+        raise RuntimeError(R.ref_last_error().decode())
+    return C
 
 
 # ----------------------------------------------------------------------------
@@ -128,6 +140,21 @@ def orc_quartet(basis, i, j, k, m):
                              exps.ctypes.data, coefs.ctypes.data, i, j, k, m, out.ctypes.data)
     assert rc == 0
     return out.reshape(nf)
+
+
+def orc_quartets(basis, quartets):
+    """Blocks of many quartets (int array [n][4] of shell indices), concatenated in
+    order, each [a][b][c][d]; OpenMP over quartets."""
+    O = restatement()
+    l, nprim, centers, exps, coefs = normalized_arrays(basis)
+    q = np.ascontiguousarray(quartets, dtype=np.int32)
+    nc = (l + 1) * (l + 2) // 2
+    sizes = nc[q[:, 0]] * nc[q[:, 1]] * nc[q[:, 2]] * nc[q[:, 3]]
+    out = np.zeros(int(sizes.sum()))
+    rc = O.orc_basis_quartets(len(l), l.ctypes.data, nprim.ctypes.data, centers.ctypes.data,
+                              exps.ctypes.data, coefs.ctypes.data, len(q), q.ctypes.data, out.ctypes.data)
+    assert rc == 0
+    return out
 
 
 def orc_schwarz(basis):

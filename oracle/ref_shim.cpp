@@ -17,6 +17,7 @@
 //   - math::rys_compute / boys_evaluate_array src/shared/math/rys_quadrature.cpp:455-513,
 //                                             src/shared/math/boys_function.cpp:253-303
 //   - FockBuilder::accumulate_symmetric       src/shared/consumers/fock_builder.cpp:123-222
+//   - math::get_cart_to_sph_matrix            include/libaccint/math/spherical_transform.hpp:20-40
 #include <libaccint/libaccint.hpp>
 #include <libaccint/engine/engine.hpp>
 #include <libaccint/consumers/fock_builder.hpp>
@@ -24,6 +25,7 @@
 #include <libaccint/kernels/eri_kernel.hpp>
 #include <libaccint/math/rys_quadrature.hpp>
 #include <libaccint/math/boys_function.hpp>
+#include <libaccint/math/spherical_transform.hpp>
 #include <libaccint/screening/schwarz_bounds.hpp>
 #include <libaccint/screening/screening_options.hpp>
 
@@ -300,5 +302,18 @@ double ref_time_quartets(void* h, const double* D, const long* quartets, long nq
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }
+
+// C_l [n_sph x n_cart] row-major of the reference (l <= 4); returns n_sph*n_cart or -1.
+int ref_cart_to_sph(int l, double* out) {
+    try {
+        const double* C = libaccint::math::get_cart_to_sph_matrix(l);
+        const int n = (2 * l + 1) * (l + 1) * (l + 2) / 2;
+        std::memcpy(out, C, sizeof(double) * n);
+        return n;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1;
+    }
+}
 
 }  // extern "C"

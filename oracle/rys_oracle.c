@@ -363,6 +363,26 @@ int orc_basis_quartet(int n, const int *l, const int *nprim, const double *ctr, 
     return rc;
 }
 
+/* Many contracted quartets (shell indices q[4t..4t+3]), blocks concatenated in
+   order into out (each [a][b][c][d]); OpenMP over quartets.  Returns 0. */
+int orc_basis_quartets(int n, const int *l, const int *nprim, const double *ctr, const double *exps,
+                       const double *coefs, long nq, const int *q, double *out) {
+    basis_t b;
+    basis_init(&b, n, l, nprim, ctr, exps, coefs);
+    long *off = malloc(sizeof(long) * (nq + 1));
+    off[0] = 0;
+    for (long t = 0; t < nq; ++t)
+        off[t + 1] = off[t] + (long)ncart(l[q[4 * t]]) * ncart(l[q[4 * t + 1]]) *
+                                  ncart(l[q[4 * t + 2]]) * ncart(l[q[4 * t + 3]]);
+    int rc = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : rc)
+    for (long t = 0; t < nq; ++t)
+        rc |= quartet(&b, q[4 * t], q[4 * t + 1], q[4 * t + 2], q[4 * t + 3], out + off[t]);
+    free(off);
+    basis_free(&b);
+    return rc;
+}
+
 /* Schwarz bounds Q[i*n+j] = sqrt(max_ab |(ab|ab)|). */
 int orc_schwarz(int n, const int *l, const int *nprim, const double *ctr, const double *exps,
                 const double *coefs, double *Q) {
