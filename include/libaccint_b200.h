@@ -122,6 +122,12 @@ typedef struct {
                           J/K then hold this rank's partial sums -- add them over
                           ranks (one all-reduce) to get the full J/K            */
   int profile;         /* 1 = time every kernel launch (lai_jk_last_profile)    */
+  int graph;           /* lai_jk_build_device only: 1 = run the build as a CUDA
+                          graph, captured on the first call for these (D, J, K,
+                          stream, fp32_cut, shard) and replayed afterwards (one
+                          launch instead of one per shell-quartet class).  Needs
+                          a non-NULL stream and profile = 0; the replays keep
+                          the FP32 cut derived from max|D| at capture time.     */
 } lai_jk_opts;
 LAI_API void lai_jk_opts_default(lai_jk_opts* opts);
 
@@ -179,6 +185,24 @@ typedef struct {
 LAI_API int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_capacity,
                                    lai_quartet_meta* meta, size_t meta_capacity,
                                    int64_t* n_quartets, int64_t* n_values);
+
+/* ---------------------------------------------------------------------------
+ * Batched engine: many independent systems (molecules, clusters) in one engine,
+ * so that every shell-quartet class of all of them runs as one persistent launch.
+ * Quartets never mix systems.  D, J and K are packed: system s's nbf_s x nbf_s
+ * block (row-major) starts at element offsets[s] (lai_engine_batch_layout).
+ * lai_jk_build_device takes packed device arrays for a batched engine; the host
+ * variant is lai_jk_build_batched.  No counterpart in the reference (one basis
+ * per Engine).  Entry points that address one basis-wide matrix (lai_jk_build,
+ * lai_engine_schwarz, lai_eri_batch_screened, work units, gradients, spherical
+ * transforms, lai_jk_build_noalloc) return LAI_ENOTSUP for a batched engine.
+ * ------------------------------------------------------------------------- */
+LAI_API int lai_engine_create_batched(int nsys, const lai_basis* const* bases, const lai_engine_opts* opts,
+                                      lai_engine** out);
+/* nsys; offsets[nsys + 1] (elements); nbf[nsys].  Any output may be NULL. */
+LAI_API int lai_engine_batch_layout(lai_engine* engine, int* nsys, int64_t* offsets, int* nbf);
+LAI_API int lai_jk_build_batched(lai_engine* engine, const double* D, double* J, double* K,
+                                 const lai_jk_opts* opts, lai_jk_report* report);
 
 /* ---------------------------------------------------------------------------
  * Work units: a caller-supplied list of shell quartets, quartets[4t..4t+3] =
@@ -270,6 +294,13 @@ LAI_API int lai_engine_sample_quartets(lai_engine* engine, int64_t n, uint64_t s
                                        int32_t* quartets);
 /* Total canonical screened quartets of the engine. */
 LAI_API int64_t lai_engine_quartet_count(lai_engine* engine);
+/* Autotuner: times every thread-per-quartet class launch of the engine under a
+ * few launch configurations (lanes per quartet 1..8, chunks per super-chunk 1, 4,
+ * 16) on the device density d_D, and keeps the fastest for later builds.
+ * ms_before/ms_after (may be NULL): summed launch times with the built-in
+ * heuristic and with the chosen configurations.  Synchronizes `stream`. */
+LAI_API int lai_engine_autotune(lai_engine* engine, const double* d_D, void* stream, double* ms_before,
+                                double* ms_after);
 /* FP64 FMA throughput of the device measured by a register-resident FMA loop
  * (TFLOP/s, 2 FLOP per FMA): the speed-of-light denominator of the FP64 path. */
 LAI_API int lai_probe_fp64_peak(int device, double* tflops);

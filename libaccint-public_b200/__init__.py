@@ -5,5 +5,6 @@ directory name is not a Python identifier).
 """
 from ._lib import LibAccIntError, lib  # noqa: F401
 from .basis import BasisSet, Shell, basis_data, cart_to_sph_matrix  # noqa: F401
-from .engine import Engine, FockBuilder, Operator, ScreeningOptions, jk, probe_fp64_peak  # noqa: F401
+from .engine import (BatchedEngine, Engine, FockBuilder, Operator, ScreeningOptions, jk,  # noqa: F401
+                     probe_fp64_peak)
 from . import autograd, molecules, workloads  # noqa: F401

@@ -26,6 +26,8 @@ EXPORTED = [
     "lai_eri_quartets", "lai_jk_accumulate_quartets", "lai_jk_accumulate_quartets_device",
     "lai_jk_accumulate_eri_batch_device",
     "lai_engine_natom", "lai_jk_gradient", "lai_jk_gradient_device",
+    "lai_engine_create_batched", "lai_engine_batch_layout", "lai_jk_build_batched",
+    "lai_engine_autotune",
 ]
 
 
@@ -42,7 +44,8 @@ class EngineOpts(ctypes.Structure):
 
 class JKOpts(ctypes.Structure):
     _fields_ = [("fp32_cut", ctypes.c_double), ("check_symmetric", ctypes.c_int),
-                ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int), ("profile", ctypes.c_int)]
+                ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int), ("profile", ctypes.c_int),
+                ("graph", ctypes.c_int)]
 
 
 class QuartetMeta(ctypes.Structure):
@@ -105,6 +108,10 @@ def lib():
         "lai_engine_natom": (I, [P]),
         "lai_jk_gradient": (I, [P, P, ctypes.c_size_t, P]),
         "lai_jk_gradient_device": (I, [P, P, P, P]),
+        "lai_engine_create_batched": (I, [I, P, ctypes.POINTER(EngineOpts), ctypes.POINTER(P)]),
+        "lai_engine_batch_layout": (I, [P, P, P, P]),
+        "lai_jk_build_batched": (I, [P, P, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKReport)]),
+        "lai_engine_autotune": (I, [P, P, P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -214,8 +214,11 @@ int build_classes(lai_engine* E) {
     c.la = la; c.lb = lb; c.Ka = Ka; c.Kb = Kb;
     return (int)keys.size() - 1;
   };
-  for (int i = 0; i < ns; ++i)
-    for (int j = 0; j <= i; ++j) {
+  // pairs within one system only (shells of a system are contiguous)
+  int sys_first = 0;
+  for (int i = 0; i < ns; ++i) {
+    if (i > 0 && sh[i].sys != sh[i - 1].sys) sys_first = i;
+    for (int j = sys_first; j <= i; ++j) {
       int a = i, b = j;
       const int Ki = (int)sh[i].exps.size(), Kj = (int)sh[j].exps.size();
       // orient: higher l first, then more primitives first
@@ -226,7 +229,9 @@ int build_classes(lai_engine* E) {
       auto& c = *E->classes[ci];
       c.sa.push_back(a); c.sb.push_back(b);
       c.fa.push_back((int)A.func); c.fb.push_back((int)B.func);
+      c.sys.push_back(A.sys);
     }
+  }
   // sort classes by key so that bra >= ket implies (la,lb) >= (lc,ld)
   std::vector<int> order(keys.size());
   std::iota(order.begin(), order.end(), 0);
@@ -286,6 +291,7 @@ int upload_class(PairClassHost& c) {
 
 int ensure_scratch(lai_engine* E, size_t doubles) {
   if (doubles <= E->scratch_doubles) return LAI_OK;
+  E->release_graph();
   LAI_CUDA_TRY(E->d_scratch.alloc(doubles * sizeof(double)));
   E->scratch_doubles = doubles;
   return LAI_OK;
@@ -294,11 +300,11 @@ int ensure_scratch(lai_engine* E, size_t doubles) {
 // Launches the kernel of the block's class.  fp32 asks for the FP32 variant; the
 // classes without one (generic kernel) run in FP64, and *ran_fp32 says which ran.
 int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs& args,
-                 bool fp32, bool* ran_fp32) {
+                 bool fp32, bool* ran_fp32, lai::LaunchTune tune) {
   const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
   if (ran_fp32) *ran_fp32 = false;
   if (lai::small_class_supported(la, lb, lc, ld)) {
-    const int rc = lai::launch_small(blk, args, E->tab, E->stream, fp32, E->num_sms);
+    const int rc = lai::launch_small(blk, args, E->tab, E->stream, fp32, E->num_sms, tune);
     if (ran_fp32) *ran_fp32 = fp32;
     if (rc < 0) return fail(LAI_ECUDA, std::string("small-class launch failed: ") +
                                            cudaGetErrorString(cudaGetLastError()));
@@ -407,22 +413,30 @@ int compute_prim_schwarz(lai_engine* E) {
 
 int sort_and_screen(lai_engine* E) {
   const int ns = (int)E->basis->shells.size();
-  E->Q_all.assign((size_t)ns * ns, 0.0);
+  const bool batched = E->nsys > 1;
+  if (!batched) E->Q_all.assign((size_t)ns * ns, 0.0);  // (a full matrix only for one system)
   double qmax = 0.0;
   for (auto& cp : E->classes)
     for (int p = 0; p < cp->n(); ++p) {
       qmax = std::max(qmax, cp->Q[p]);
-      E->Q_all[(size_t)cp->sa[p] * ns + cp->sb[p]] = cp->Q[p];
-      E->Q_all[(size_t)cp->sb[p] * ns + cp->sa[p]] = cp->Q[p];
+      if (!batched) {
+        E->Q_all[(size_t)cp->sa[p] * ns + cp->sb[p]] = cp->Q[p];
+        E->Q_all[(size_t)cp->sb[p] * ns + cp->sa[p]] = cp->Q[p];
+      }
     }
   for (auto& cp : E->classes) {
     auto& c = *cp;
     const int n = c.n();
-    std::vector<int> idx(n);
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return c.Q[x] > c.Q[y]; });
-    int keep = 0;
-    while (keep < n && c.Q[idx[keep]] * qmax >= E->thr) ++keep;
+    // pairs ordered by system, then by Schwarz bound (descending); pairs that pass
+    // with no partner dropped -- each system's kept pairs are a prefix of its segment
+    std::vector<int> idx;
+    idx.reserve(n);
+    for (int i = 0; i < n; ++i)
+      if (c.Q[i] * qmax >= E->thr) idx.push_back(i);
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+      return c.sys[x] != c.sys[y] ? c.sys[x] < c.sys[y] : c.Q[x] > c.Q[y];
+    });
+    const int keep = (int)idx.size();
     const int Kab = c.Ka * c.Kb;
     auto perm = [&](const std::vector<int>& v) {
       std::vector<int> o(keep);
@@ -451,8 +465,16 @@ int sort_and_screen(lai_engine* E) {
       c.qprim_max = std::max(c.qprim_max, qat(0));
     }
     c.sa = perm(c.sa); c.sb = perm(c.sb); c.fa = perm(c.fa); c.fb = perm(c.fb);
+    c.sys = perm(c.sys);
     c.Q = std::move(Q); c.AB = std::move(AB); c.prim = std::move(prim);
+    c.seg.assign(E->nsys + 1, 0);
+    for (int i = 0, s = 0; s <= E->nsys; ++s) {
+      while (i < keep && c.sys[i] < s) ++i;
+      c.seg[s] = i;
+    }
+    c.batched = batched;
     if (int rc = upload_class(c)) return rc;
+    if (batched) LAI_CUDA_TRY(upload(c.d_sys, c.sys));
   }
   // quartet blocks
   const int nc = (int)E->classes.size();
@@ -466,19 +488,24 @@ int sort_and_screen(lai_engine* E) {
       blk->ket = B;
       blk->offsets.resize(ca.n() + 1);
       blk->offsets[0] = 0;
+      if (batched) blk->qbegin.resize(ca.n());
       for (int p = 0; p < ca.n(); ++p) {
-        // largest prefix of the ket list with Q_p * Q_q >= thr
-        int lo = 0, hi = cb.n();
+        // largest prefix of the bra pair's system segment of the ket list with
+        // Q_p * Q_q >= thr (the whole list for a single system)
+        const int s0 = cb.seg[ca.sys[p]], s1 = cb.seg[ca.sys[p] + 1];
+        int lo = s0, hi = s1;
         while (lo < hi) {
           const int mid = (lo + hi) / 2;
           if (ca.Q[p] * cb.Q[mid] >= E->thr) lo = mid + 1; else hi = mid;
         }
-        int cnt = lo;
-        if (A == B) cnt = std::min(cnt, p + 1);
+        int cnt = lo - s0;
+        if (A == B) cnt = std::min(cnt, p - s0 + 1);  // canonical q <= p (same segment)
         blk->offsets[p + 1] = blk->offsets[p] + cnt;
+        if (batched) blk->qbegin[p] = s0;
       }
       blk->total = blk->offsets[ca.n()];
       if (blk->total == 0) continue;
+      if (batched) LAI_CUDA_TRY(upload(blk->d_qbegin, blk->qbegin));
       blk->alg_flops = alg_work(ca.la, ca.lb, cb.la, cb.lb, ca.Ka, ca.Kb, cb.Ka, cb.Kb);
       blk->flops_per_prim = alg_per_prim(ca.la, ca.lb, cb.la, cb.lb);
       blk->flops_per_quartet = alg_per_quartet(ca.la, ca.lb, cb.la, cb.lb);
@@ -493,7 +520,7 @@ lai::QuartetBlock make_block(const lai_engine* E, const ClassPairBlock& b) {
   q.bra = E->classes[b.bra]->view();
   q.ket = E->classes[b.ket]->view();
   q.offsets = b.d_offsets.as<int64_t>();
-  q.qbegin = nullptr;
+  q.qbegin = b.qbegin.empty() ? nullptr : b.d_qbegin.as<int>();
   q.total = b.total;
   q.same_class = (b.bra == b.ket);
   return q;
@@ -526,9 +553,16 @@ int device_absmax(lai_engine* E, const double* x, size_t n, cudaStream_t stream,
   return LAI_OK;
 }
 
+// Elements of the engine's D/J/K arrays: nbf^2, or the packed blocks of a batched engine.
+size_t engine_mat_elems(const lai_engine* E) {
+  if (E->nsys > 1) return (size_t)E->sys_off[E->nsys];
+  return (size_t)E->basis->nbf * (size_t)E->basis->nbf;
+}
+
 // Builds (once per cut value) the FP64/FP32 split of every block.
 int build_split(lai_engine* E, double cut) {
   if (E->split_cut == cut) return LAI_OK;
+  E->release_graph();  // a captured graph points into the buffers rebuilt here
   E->split_cut = -1.0;
   for (auto& bp : E->blocks) {
     auto& b = *bp;
@@ -540,14 +574,15 @@ int build_split(lai_engine* E, double cut) {
     o64[0] = o32[0] = 0;
     for (int p = 0; p < n; ++p) {
       const int64_t cnt = b.offsets[p + 1] - b.offsets[p];
+      const int base = b.qbegin.empty() ? 0 : b.qbegin[p];  // first ket of the bra's range
       int lo = 0, hi = (int)cnt;  // first ket with Q_p Q_q < cut
       while (lo < hi) {
         const int mid = (lo + hi) / 2;
-        if (ca.Q[p] * cb.Q[mid] >= cut) lo = mid + 1; else hi = mid;
+        if (ca.Q[p] * cb.Q[base + mid] >= cut) lo = mid + 1; else hi = mid;
       }
       o64[p + 1] = o64[p] + lo;
       o32[p + 1] = o32[p] + (cnt - lo);
-      qb32[p] = lo;
+      qb32[p] = base + lo;
     }
     b.total64 = o64[n];
     b.total32 = o32[n];
@@ -559,13 +594,39 @@ int build_split(lai_engine* E, double cut) {
   return LAI_OK;
 }
 
+// J = J' + J'^T, K = K' + K'^T on every system block of a batched engine's packed
+// matrices (block s = nbf_s x nbf_s at element offset off[s]).
+__global__ void symmetrize_batched_kernel(const double* __restrict__ Jp, const double* __restrict__ Kp,
+                                          double* __restrict__ J, double* __restrict__ K,
+                                          const int64_t* __restrict__ off, const int* __restrict__ nbfs,
+                                          int nsys) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= off[nsys]) return;
+  int lo = 0, hi = nsys;  // off[lo] <= idx < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= idx) lo = mid; else hi = mid;
+  }
+  const int n = nbfs[lo];
+  const int64_t l = idx - off[lo];
+  const int i = (int)(l / n), j = (int)(l - (int64_t)i * n);
+  const int64_t tr = off[lo] + (int64_t)j * n + i;
+  J[idx] = Jp[idx] + Jp[tr];
+  K[idx] = Kp[idx] + Kp[tr];
+}
+
+// forced_cut >= 0: use this Schwarz cut for the FP32 split instead of deriving it
+// from max|D| (which synchronizes the stream; not allowed while capturing a graph).
 int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t stream,
-           const lai_jk_opts& o, lai_jk_report* rep, bool timed) {
+           const lai_jk_opts& o, lai_jk_report* rep, bool timed, double forced_cut = -1.0) {
   const int nbf = (int)E->basis->nbf;
-  const size_t bytes = sizeof(double) * (size_t)nbf * nbf;
+  const bool batched = E->nsys > 1;
+  const size_t elems = engine_mat_elems(E);
+  const size_t bytes = sizeof(double) * elems;
   if (o.shard_count < 1 || o.shard_index < 0 || o.shard_index >= o.shard_count)
     return fail(LAI_EINVAL, "lai_jk: bad shard_index/shard_count");
   if (E->d_Jp.bytes < bytes) {
+    E->release_graph();
     LAI_CUDA_TRY(E->d_Jp.alloc(bytes));
     LAI_CUDA_TRY(E->d_Kp.alloc(bytes));
   }
@@ -581,6 +642,10 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
   args.nbf = nbf;
   args.mode = lai::MODE_JK;
   args.prim_eps = E->prim_eps;
+  if (batched) {
+    args.sys_off = E->d_sys_off.as<int64_t>();
+    args.sys_nbf = E->d_sys_nbf.as<int>();
+  }
   int launches = 0;
   int64_t nq = 0, nq32 = 0;
   double flops = 0;
@@ -588,10 +653,10 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
   // Schwarz cut fp32_cut / max|D| is rounded down to a power of two (conservative:
   // fewer FP32 quartets), so that the split, built on the host, is rebuilt only
   // when max|D| moves past a power of two.
-  double cut = 0.0;
-  if (o.fp32_cut > 0.0) {
+  double cut = forced_cut >= 0.0 ? forced_cut : 0.0;
+  if (o.fp32_cut > 0.0 && forced_cut < 0.0) {
     double maxd = 0.0;
-    if (int rc = device_absmax(E, dD, (size_t)nbf * nbf, stream, &maxd)) { E->stream = saved; return rc; }
+    if (int rc = device_absmax(E, dD, elems, stream, &maxd)) { E->stream = saved; return rc; }
     if (maxd > 0.0 && std::isfinite(maxd)) cut = std::exp2(std::floor(std::log2(o.fp32_cut / maxd)));
   }
   const bool mixed = cut > 0.0;
@@ -624,7 +689,7 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
       if (mixed) {
         total = part == 0 ? bp.total64 : bp.total32;
         q.offsets = (part == 0 ? bp.d_off64 : bp.d_off32).as<int64_t>();
-        q.qbegin = part == 0 ? nullptr : bp.d_qb32.as<int>();
+        if (part == 1) q.qbegin = bp.d_qb32.as<int>();  // the FP64 part keeps the block's ket starts
       }
       // this shard's contiguous slice of the part
       const int64_t lo = total * o.shard_index / o.shard_count;
@@ -635,7 +700,7 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
       args.prim_count = o.profile ? E->d_prof_prims.as<unsigned long long>() + E->prof_n : nullptr;
       if (o.profile) LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n], stream));
       bool ran32 = false;
-      if (int rc = launch_block(E, q, args, part == 1, &ran32)) { E->stream = saved; return rc; }
+      if (int rc = launch_block(E, q, args, part == 1, &ran32, bp.tune)) { E->stream = saved; return rc; }
       if (o.profile) {
         LAI_CUDA_TRY(cudaEventRecord(E->prof_ev[2 * E->prof_n + 1], stream));
         E->prof_block.push_back((int)b);
@@ -648,10 +713,15 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
       flops += bp.alg_flops * (double)(hi - lo);
     }
   }
-  const int64_t nn = (int64_t)nbf * nbf;
+  const int64_t nn = (int64_t)elems;
   if (nn > 0) {
-    symmetrize_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(
-        E->d_Jp.as<double>(), E->d_Kp.as<double>(), dJ, dK, nbf);
+    if (batched)
+      symmetrize_batched_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(
+          E->d_Jp.as<double>(), E->d_Kp.as<double>(), dJ, dK, E->d_sys_off.as<int64_t>(),
+          E->d_sys_nbf.as<int>(), E->nsys);
+    else
+      symmetrize_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(
+          E->d_Jp.as<double>(), E->d_Kp.as<double>(), dJ, dK, nbf);
     ++launches;
   }
   LAI_CUDA_TRY(cudaGetLastError());
@@ -710,11 +780,18 @@ void lai_jk_opts_default(lai_jk_opts* opts) {
   opts->shard_index = 0;
   opts->shard_count = 1;
   opts->profile = 0;
+  opts->graph = 0;
 }
 
-int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_engine** out) {
-  if (!out || !basis) return fail(LAI_EINVAL, "lai_engine_create: null argument");
-  *out = nullptr;
+}  // extern "C"
+
+namespace lai {
+namespace host {
+
+// Engine over `basis`; for a batched engine, `merged` is the concatenation of the
+// systems' shells (each tagged with its system) and sys_nbf their function counts.
+int create_engine(const lai_basis* basis, std::unique_ptr<lai_basis> merged, const std::vector<int>& sys_nbf,
+                  const lai_engine_opts* opts, lai_engine** out) {
   lai_engine_opts o;
   lai_engine_opts_default(&o);
   if (opts) o = *opts;
@@ -724,7 +801,19 @@ int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_e
   if (o.device < 0 || o.device >= ndev) return fail(LAI_EINVAL, "lai_engine_create: bad device");
   LAI_CUDA_TRY(cudaSetDevice(o.device));
   auto E = std::make_unique<lai_engine>();
-  E->basis = basis;
+  if (merged) {
+    E->merged = std::move(merged);
+    E->basis = E->merged.get();
+    E->nsys = (int)sys_nbf.size();
+    E->sys_nbf = sys_nbf;
+    E->sys_off.assign(E->nsys + 1, 0);
+    for (int i = 0; i < E->nsys; ++i) E->sys_off[i + 1] = E->sys_off[i] + (int64_t)sys_nbf[i] * sys_nbf[i];
+    LAI_CUDA_TRY(upload(E->d_sys_nbf, E->sys_nbf));
+    LAI_CUDA_TRY(upload(E->d_sys_off, E->sys_off));
+  } else {
+    E->basis = basis;
+  }
+  basis = E->basis;
   E->device = o.device;
   E->thr = o.schwarz_threshold;
   E->prim_eps = o.prim_threshold < 0.0 ? 1e-3 * o.schwarz_threshold : o.prim_threshold;
@@ -756,6 +845,48 @@ int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_e
   return LAI_OK;
 }
 
+}  // namespace host
+}  // namespace lai
+
+extern "C" {
+
+int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_engine** out) {
+  if (!out || !basis) return fail(LAI_EINVAL, "lai_engine_create: null argument");
+  *out = nullptr;
+  return create_engine(basis, nullptr, {}, opts, out);
+}
+
+int lai_engine_create_batched(int nsys, const lai_basis* const* bases, const lai_engine_opts* opts,
+                              lai_engine** out) {
+  if (!out || nsys < 1 || !bases) return fail(LAI_EINVAL, "lai_engine_create_batched: null argument");
+  *out = nullptr;
+  auto merged = std::make_unique<lai_basis>();
+  std::vector<int> nbf(nsys);
+  for (int s = 0; s < nsys; ++s) {
+    if (!bases[s]) return fail(LAI_EINVAL, "lai_engine_create_batched: null basis");
+    for (const HostShell& sh : bases[s]->shells) {
+      merged->shells.push_back(sh);
+      merged->shells.back().sys = s;  // func stays local to the system
+    }
+    nbf[s] = (int)bases[s]->nbf;
+  }
+  merged->nbf = 0;  // no single matrix size: D/J/K are packed per system
+  return create_engine(nullptr, std::move(merged), nbf, opts, out);
+}
+
+int lai_engine_batch_layout(lai_engine* engine, int* nsys, int64_t* offsets, int* nbf) {
+  if (!engine) return fail(LAI_EINVAL, "lai_engine_batch_layout: null engine");
+  if (nsys) *nsys = engine->nsys;
+  if (engine->nsys == 1) {
+    if (offsets) { offsets[0] = 0; offsets[1] = (int64_t)engine->basis->nbf * engine->basis->nbf; }
+    if (nbf) nbf[0] = (int)engine->basis->nbf;
+    return LAI_OK;
+  }
+  if (offsets) std::copy(engine->sys_off.begin(), engine->sys_off.end(), offsets);
+  if (nbf) std::copy(engine->sys_nbf.begin(), engine->sys_nbf.end(), nbf);
+  return LAI_OK;
+}
+
 void lai_engine_destroy(lai_engine* engine) {
   if (engine) {
     cudaSetDevice(engine->device);
@@ -764,6 +895,7 @@ void lai_engine_destroy(lai_engine* engine) {
 }
 
 int lai_engine_schwarz(lai_engine* engine, double* Q) {
+  if (engine && engine->nsys > 1) return fail(LAI_ENOTSUP, "lai_engine_schwarz: not available for a batched engine");
   if (!engine || !Q) return fail(LAI_EINVAL, "lai_engine_schwarz: null argument");
   std::copy(engine->Q_all.begin(), engine->Q_all.end(), Q);
   return LAI_OK;
@@ -777,13 +909,44 @@ int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d_J, doub
   if (opts) o = *opts;
   if (!(o.fp32_cut >= 0.0)) return fail(LAI_EINVAL, "lai_jk_build_device: fp32_cut must be >= 0");
   LAI_CUDA_TRY(cudaSetDevice(engine->device));
-  return run_jk(engine, d_D, d_J, d_K, (cudaStream_t)stream, o, report, false);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!o.graph) return run_jk(engine, d_D, d_J, d_K, s, o, report, false);
+  if (!s || o.profile) return fail(LAI_EINVAL, "lai_jk_build_device: graph mode needs a stream and profile = 0");
+  lai_engine::GraphKey key{d_D, d_J, d_K, s, o.fp32_cut, o.shard_index, o.shard_count};
+  if (engine->graph_exec && engine->graph_key == key) {
+    LAI_CUDA_TRY(cudaGraphLaunch(engine->graph_exec, s));
+    if (report) *report = engine->graph_report;
+    return LAI_OK;
+  }
+  // First call: an ordinary build (allocations, the FP32 split and its cut), whose
+  // result is this call's; then the same launch sequence captured for the replays.
+  lai_jk_report rep{};
+  if (int rc = run_jk(engine, d_D, d_J, d_K, s, o, &rep, false)) return rc;
+  engine->release_graph();
+  cudaGraph_t graph = nullptr;
+  LAI_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  lai_jk_report rep2{};
+  const int rc = run_jk(engine, d_D, d_J, d_K, s, o, &rep2, false, rep.fp32_schwarz_cut);
+  const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  LAI_CUDA_TRY(ce);
+  const cudaError_t ie = cudaGraphInstantiate(&engine->graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  LAI_CUDA_TRY(ie);
+  engine->graph_key = key;
+  engine->graph_report = rep;
+  if (report) *report = rep;
+  return LAI_OK;
 }
 
 int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double* J, double* K,
                  const lai_jk_opts* opts, lai_jk_report* report) {
   auto t0 = std::chrono::steady_clock::now();
   if (!engine || !D || !J || !K) return fail(LAI_EINVAL, "lai_jk_build: null argument");
+  if (engine->nsys > 1) return fail(LAI_EINVAL, "lai_jk_build: batched engine (use lai_jk_build_batched)");
   if ((long)nbf != engine->basis->nbf)
     return fail(LAI_EINVAL, "lai_jk_build: nbf mismatch (expected " +
                                 std::to_string(engine->basis->nbf) + ", got " +
@@ -823,9 +986,42 @@ int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double* J, dou
   return LAI_OK;
 }
 
+int lai_jk_build_batched(lai_engine* engine, const double* D, double* J, double* K, const lai_jk_opts* opts,
+                         lai_jk_report* report) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (!engine || !D || !J || !K) return fail(LAI_EINVAL, "lai_jk_build_batched: null argument");
+  lai_jk_opts o;
+  lai_jk_opts_default(&o);
+  if (opts) o = *opts;
+  if (!(o.fp32_cut >= 0.0)) return fail(LAI_EINVAL, "lai_jk_build_batched: fp32_cut must be >= 0");
+  LAI_CUDA_TRY(cudaSetDevice(engine->device));
+  const size_t bytes = sizeof(double) * engine_mat_elems(engine);
+  if (engine->d_D.bytes < bytes) {
+    LAI_CUDA_TRY(engine->d_D.alloc(bytes));
+    LAI_CUDA_TRY(engine->d_J.alloc(bytes));
+    LAI_CUDA_TRY(engine->d_K.alloc(bytes));
+  }
+  cudaStream_t s = engine->stream;
+  LAI_CUDA_TRY(cudaMemcpyAsync(engine->d_D.p, D, bytes, cudaMemcpyHostToDevice, s));
+  if (int rc = run_jk(engine, engine->d_D.as<double>(), engine->d_J.as<double>(), engine->d_K.as<double>(), s, o,
+                      report, true))
+    return rc;
+  LAI_CUDA_TRY(cudaMemcpyAsync(J, engine->d_J.p, bytes, cudaMemcpyDeviceToHost, s));
+  LAI_CUDA_TRY(cudaMemcpyAsync(K, engine->d_K.p, bytes, cudaMemcpyDeviceToHost, s));
+  LAI_CUDA_TRY(cudaStreamSynchronize(s));
+  if (report) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, engine->ev0, engine->ev1);
+    report->seconds_device = ms * 1e-3;
+    report->seconds_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return LAI_OK;
+}
+
 int lai_eri_batch_screened(lai_engine* engine, double* out, size_t out_capacity,
                            lai_quartet_meta* meta, size_t meta_capacity, int64_t* n_quartets,
                            int64_t* n_values) {
+  if (engine && engine->nsys > 1) return fail(LAI_ENOTSUP, "lai_eri_batch_screened: not available for a batched engine");
   if (!engine) return fail(LAI_EINVAL, "lai_eri_batch_screened: null engine");
   int64_t nq = 0, nv = 0;
   std::vector<int64_t> vals_per(engine->blocks.size());
@@ -923,6 +1119,7 @@ int64_t lai_engine_quartet_count(lai_engine* engine) {
 }
 
 int lai_engine_sample_quartets(lai_engine* engine, int64_t n, uint64_t seed, int32_t* quartets) {
+  if (engine && engine->nsys > 1) return fail(LAI_ENOTSUP, "lai_engine_sample_quartets: not available for a batched engine");
   if (!engine || n < 0 || (n > 0 && !quartets)) return fail(LAI_EINVAL, "lai_engine_sample_quartets");
   std::vector<int64_t> pref(engine->blocks.size() + 1, 0);
   for (size_t b = 0; b < engine->blocks.size(); ++b) pref[b + 1] = pref[b] + engine->blocks[b]->total;
@@ -943,6 +1140,83 @@ int lai_engine_sample_quartets(lai_engine* engine, int64_t n, uint64_t seed, int
     quartets[4 * i + 2] = cb.sa[q];
     quartets[4 * i + 3] = cb.sb[q];
   }
+  return LAI_OK;
+}
+
+int lai_engine_autotune(lai_engine* engine, const double* d_D, void* stream, double* ms_before,
+                        double* ms_after) {
+  if (!engine || !d_D) return fail(LAI_EINVAL, "lai_engine_autotune: null argument");
+  LAI_CUDA_TRY(cudaSetDevice(engine->device));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // one ordinary build first: allocations and accumulators
+  lai_jk_opts o;
+  lai_jk_opts_default(&o);
+  const size_t elems = engine_mat_elems(engine);
+  DevBuf dJ, dK;
+  LAI_CUDA_TRY(dJ.alloc(sizeof(double) * elems));
+  LAI_CUDA_TRY(dK.alloc(sizeof(double) * elems));
+  if (int rc = run_jk(engine, d_D, dJ.as<double>(), dK.as<double>(), s, o, nullptr, false)) return rc;
+  engine->release_graph();
+  cudaEvent_t e0, e1;
+  LAI_CUDA_TRY(cudaEventCreate(&e0));
+  LAI_CUDA_TRY(cudaEventCreate(&e1));
+  lai::JKArgs args{};
+  args.D = d_D;
+  args.J = engine->d_Jp.as<double>();
+  args.K = engine->d_Kp.as<double>();
+  args.nbf = (int)engine->basis->nbf;
+  args.mode = lai::MODE_JK;
+  args.prim_eps = engine->prim_eps;
+  if (engine->nsys > 1) {
+    args.sys_off = engine->d_sys_off.as<int64_t>();
+    args.sys_nbf = engine->d_sys_nbf.as<int>();
+  }
+  cudaStream_t saved = engine->stream;
+  engine->stream = s;
+  double before = 0.0, after = 0.0;
+  int rc = LAI_OK;
+  auto time_launch = [&](const lai::QuartetBlock& q, lai::LaunchTune t, float* ms) -> int {
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {  // the first run warms caches, the minimum counts
+      if (cudaEventRecord(e0, s) != cudaSuccess) return LAI_ECUDA;
+      if (int r = launch_block(engine, q, args, false, nullptr, t)) return r;
+      if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) return LAI_ECUDA;
+      float m = 0;
+      cudaEventElapsedTime(&m, e0, e1);
+      best = std::min(best, m);
+    }
+    *ms = best;
+    return LAI_OK;
+  };
+  for (auto& bp : engine->blocks) {
+    const lai::QuartetBlock q = make_block(engine, *bp);
+    bp->tune = lai::LaunchTune{};
+    float base = 0;
+    if ((rc = time_launch(q, bp->tune, &base))) break;
+    before += base;
+    if (!lai::small_class_supported(q.bra.la, q.bra.lb, q.ket.la, q.ket.lb)) {
+      after += base;
+      continue;
+    }
+    const int Kab = q.bra.Ka * q.bra.Kb;
+    lai::LaunchTune best = bp->tune;
+    float best_ms = base;
+    for (int ps = 1; ps <= 8 && ps < 2 * Kab; ps <<= 1)
+      for (int ks : {1, 4, 16}) {
+        float m = 0;
+        if ((rc = time_launch(q, lai::LaunchTune{ps, ks}, &m))) break;
+        if (m < 0.98f * best_ms) { best_ms = m; best = lai::LaunchTune{ps, ks}; }
+      }
+    if (rc) break;
+    bp->tune = best;
+    after += best_ms;
+  }
+  engine->stream = saved;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return fail(rc, "lai_engine_autotune: a timing launch failed");
+  if (ms_before) *ms_before = before;
+  if (ms_after) *ms_after = after;
   return LAI_OK;
 }
 
@@ -988,6 +1262,7 @@ int engine_nbf(const lai_engine* E) { return (int)E->basis->nbf; }
 double engine_prim_eps(const lai_engine* E) { return E->prim_eps; }
 RysTablesView engine_tables(const lai_engine* E) { return E->tab; }
 const lai_basis* engine_basis(const lai_engine* E) { return E->basis; }
+int engine_nsys(const lai_engine* E) { return E->nsys; }
 int engine_block_count(const lai_engine* E) { return (int)E->blocks.size(); }
 QuartetBlock engine_block(const lai_engine* E, int i) { return make_block(E, *E->blocks[i]); }
 void engine_set_error(const char* msg) { g_last_error = msg; }

@@ -12,6 +12,7 @@
 
 #include "../../include/libaccint_b200.h"
 #include "eri_device.cuh"
+#include "eri_kernels.h"
 
 namespace lai {
 namespace host {
@@ -62,7 +63,8 @@ struct HostShell {
   std::vector<double> exps_all, coefs_all;  // normalized, all primitives as given
   std::vector<double> exps, coefs;          // nonzero-coefficient primitives only
   int atom;
-  long func;
+  long func;     // first function of the shell within its system
+  int sys = 0;   // system index (batched engines merge independent systems)
 };
 
 struct lai_basis {
@@ -77,12 +79,15 @@ struct PairClassHost {
   int la, lb, Ka, Kb;
   double qprim_max = 0.0;
   std::vector<int> sa, sb, fa, fb;  // shell and function indices (oriented)
+  std::vector<int> sys;             // system of each pair (batched engines)
+  std::vector<int> seg;             // [nsys + 1] first pair of each system (pairs sorted by system)
   std::vector<double> Q;
   std::vector<double> AB;          // SoA [3][n]
   std::vector<double> prim;        // SoA [PF_COUNT][Kab][n]
   int n() const { return (int)sa.size(); }
   // device copies
-  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_prim;
+  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_prim, d_sys;
+  bool batched = false;             // d_sys is set (more than one system)
   lai::PairClassDev view() const {
     lai::PairClassDev v;
     v.la = la; v.lb = lb; v.Ka = Ka; v.Kb = Kb; v.npairs = n();
@@ -90,6 +95,7 @@ struct PairClassHost {
     v.func_a = d_fa.as<int>(); v.func_b = d_fb.as<int>();
     v.Q = d_Q.as<double>(); v.AB = d_AB.as<double>(); v.prim = d_prim.as<double>();
     v.qprim_max = qprim_max;
+    v.sys = batched ? d_sys.as<int>() : nullptr;
     return v;
   }
 };
@@ -98,6 +104,8 @@ struct ClassPairBlock {
   int bra, ket;                 // class indices, bra >= ket
   std::vector<int64_t> offsets; // host copy
   DevBuf d_offsets;
+  std::vector<int> qbegin;      // first ket of each bra pair (batched engines: its system's segment)
+  DevBuf d_qbegin;              // empty for a single system (every ket range starts at 0)
   int64_t total = 0;
   double alg_flops = 0;         // per quartet of this block (all nonzero primitives)
   double flops_per_prim = 0;    // per primitive quartet
@@ -108,6 +116,7 @@ struct ClassPairBlock {
   // qbegin32[p] its first ket).
   int64_t total64 = 0, total32 = 0;
   DevBuf d_off64, d_off32, d_qb32;
+  lai::LaunchTune tune;         // launch parameters chosen by lai_engine_autotune (0 = heuristic)
 };
 
 }  // namespace host
@@ -115,6 +124,13 @@ struct ClassPairBlock {
 
 struct lai_engine {
   const lai_basis* basis = nullptr;
+  // batched engines: the merged basis (owned) and the per-system layout of the
+  // packed D/J/K arrays (block s = nbf_s x nbf_s at element offset sys_off[s])
+  std::unique_ptr<lai_basis> merged;
+  int nsys = 1;
+  std::vector<int> sys_nbf;
+  std::vector<int64_t> sys_off;   // [nsys + 1]
+  lai::host::DevBuf d_sys_nbf, d_sys_off;
   int device = 0;
   int num_sms = 148;
   double thr = 1e-12;
@@ -133,6 +149,26 @@ struct lai_engine {
   lai::host::DevBuf d_absmax;
   lai::host::DevBuf d_shell_atom;  // [nshell] atom of each shell (gradients)
   int natom = -1;
+  // CUDA graph of one device build (lai_jk_opts.graph) and what it was captured for
+  struct GraphKey {
+    const double* D;
+    double* J;
+    double* K;
+    cudaStream_t stream;
+    double fp32_cut;
+    int shard_index, shard_count;
+    bool operator==(const GraphKey& o) const {
+      return D == o.D && J == o.J && K == o.K && stream == o.stream && fp32_cut == o.fp32_cut &&
+             shard_index == o.shard_index && shard_count == o.shard_count;
+    }
+  };
+  cudaGraphExec_t graph_exec = nullptr;
+  GraphKey graph_key{};
+  lai_jk_report graph_report{};
+  void release_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+  }
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // per-launch profile of the last build with opts.profile
   std::vector<cudaEvent_t> prof_ev;
@@ -141,6 +177,7 @@ struct lai_engine {
   lai::host::DevBuf d_prof_prims;
   int prof_n = 0;
   ~lai_engine() {
+    release_graph();
     for (auto e : prof_ev) cudaEventDestroy(e);
     classes.clear();
     blocks.clear();
@@ -157,7 +194,7 @@ namespace host {
 void fill_pair_data(const lai_basis* basis, PairClassHost& c);
 int upload_class(PairClassHost& c);
 int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs& args,
-                 bool fp32 = false, bool* ran_fp32 = nullptr);
+                 bool fp32 = false, bool* ran_fp32 = nullptr, lai::LaunchTune tune = lai::LaunchTune{});
 lai::QuartetBlock make_block(const lai_engine* E, const ClassPairBlock& b);
 int ensure_scratch(lai_engine* E, size_t doubles);
 double alg_work(int la, int lb, int lc, int ld, int Ka, int Kb, int Kc, int Kd);

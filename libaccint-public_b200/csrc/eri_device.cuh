@@ -95,7 +95,32 @@ struct JKArgs {
   unsigned int* status;  // device status word (0 = ok)
   double prim_eps;       // skip primitive quartets with q_ab * q_cd < prim_eps (0 = none)
   unsigned long long* prim_count;  // optional: += primitive quartets executed by the launch
+  // batched engines (many independent systems): D, J and K hold one nbf_s x nbf_s
+  // block per system, block s at element offset sys_off[s]; function indices are
+  // local to the system.  nullptr for a single system.
+  const int64_t* sys_off;
+  const int* sys_nbf;
 };
+
+// The density and Fock-matrix blocks of the system quartet (p, .) belongs to.
+struct SysMats {
+  const double* D;
+  double* J;
+  double* K;
+  int nbf;
+};
+__device__ __forceinline__ SysMats sys_mats(const JKArgs& args, const QuartetBlock& blk, int p) {
+  SysMats m{args.D, args.J, args.K, args.nbf};
+  if (blk.bra.sys) {
+    const int s = __ldg(blk.bra.sys + p);
+    const int64_t o = __ldg(args.sys_off + s);
+    m.D += o;
+    m.J += o;
+    m.K += o;
+    m.nbf = __ldg(args.sys_nbf + s);
+  }
+  return m;
+}
 
 // One ket primitive pair's data, loaded a loop iteration ahead of its use so the
 // global-memory latency overlaps the previous primitive's arithmetic (fields a

@@ -334,33 +334,34 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
 
     // ---- digestion setup ----
     const double sym = quartet_weight(blk, p, q);
+    const SysMats mats = sys_mats(args, blk, p);
     if (args.mode == MODE_JK) {
-      const int nbf = args.nbf;
+      const int nbf = mats.nbf;
       for (int i = lane; i < g.na * g.nb; i += 32) {
         const int a = i / g.nb, b = i - a * g.nb;
-        Dij[i] = __ldg(args.D + (size_t)(fa + a) * nbf + fb + b);
+        Dij[i] = __ldg(mats.D + (size_t)(fa + a) * nbf + fb + b);
       }
       for (int i = lane; i < ncd; i += 32) {
         const int c = i / g.nd, d = i - c * g.nd;
-        Dkl[i] = __ldg(args.D + (size_t)(fc + c) * nbf + fd + d);
+        Dkl[i] = __ldg(mats.D + (size_t)(fc + c) * nbf + fd + d);
         Akl[i] = 0.0;
       }
       for (int i = lane; i < g.na * g.nc; i += 32) {
         const int a = i / g.nc, c = i - a * g.nc;
-        Dik[i] = __ldg(args.D + (size_t)(fa + a) * nbf + fc + c);
+        Dik[i] = __ldg(mats.D + (size_t)(fa + a) * nbf + fc + c);
       }
       for (int i = lane; i < g.na * g.nd; i += 32) {
         const int a = i / g.nd, d = i - a * g.nd;
-        Dil[i] = __ldg(args.D + (size_t)(fa + a) * nbf + fd + d);
+        Dil[i] = __ldg(mats.D + (size_t)(fa + a) * nbf + fd + d);
       }
       for (int i = lane; i < g.nb * g.nc; i += 32) {
         const int b = i / g.nc, c = i - b * g.nc;
-        Djk[i] = __ldg(args.D + (size_t)(fb + b) * nbf + fc + c);
+        Djk[i] = __ldg(mats.D + (size_t)(fb + b) * nbf + fc + c);
         Ajk[i] = 0.0;
       }
       for (int i = lane; i < g.nb * g.nd; i += 32) {
         const int b = i / g.nd, d = i - b * g.nd;
-        Djl[i] = __ldg(args.D + (size_t)(fb + b) * nbf + fd + d);
+        Djl[i] = __ldg(mats.D + (size_t)(fb + b) * nbf + fd + d);
         Ajl[i] = 0.0;
       }
     }
@@ -405,25 +406,25 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
       }
       __syncwarp();
       if (args.mode == MODE_JK) {
-        const int nbf = args.nbf;
+        const int nbf = mats.nbf;
         for (int i = lane; i < g.nb + g.nc + g.nd; i += 32) {
           if (i < g.nb) {  // J_ij[a][b] += 2 s sum_cd O[b][c][d] D_kl[c][d]
             const int b = i;
             double v = 0.0;
             for (int x = 0; x < ncd; ++x) v += O[b * ncd + x] * Dkl[x];
-            atomicAdd(args.J + (size_t)(fa + a) * nbf + fb + b, 2.0 * sym * v);
+            atomicAdd(mats.J + (size_t)(fa + a) * nbf + fb + b, 2.0 * sym * v);
           } else if (i < g.nb + g.nc) {  // K_ik[a][c] += s sum_bd O[b][c][d] D_jl[b][d]
             const int c = i - g.nb;
             double v = 0.0;
             for (int b = 0; b < g.nb; ++b)
               for (int d = 0; d < g.nd; ++d) v += O[b * ncd + c * g.nd + d] * Djl[b * g.nd + d];
-            atomicAdd(args.K + (size_t)(fa + a) * nbf + fc + c, sym * v);
+            atomicAdd(mats.K + (size_t)(fa + a) * nbf + fc + c, sym * v);
           } else {  // K_il[a][d] += s sum_bc O[b][c][d] D_jk[b][c]
             const int d = i - g.nb - g.nc;
             double v = 0.0;
             for (int b = 0; b < g.nb; ++b)
               for (int c = 0; c < g.nc; ++c) v += O[b * ncd + c * g.nd + d] * Djk[b * g.nc + c];
-            atomicAdd(args.K + (size_t)(fa + a) * nbf + fd + d, sym * v);
+            atomicAdd(mats.K + (size_t)(fa + a) * nbf + fd + d, sym * v);
           }
         }
         for (int i = lane; i < ncd; i += 32) {  // J_kl[c][d] partial: sum_b O D_ij[a][b]
@@ -447,18 +448,18 @@ __global__ void __launch_bounds__(128) eri_generic_kernel(QuartetBlock blk, JKAr
       __syncwarp();
     }
     if (args.mode == MODE_JK) {
-      const int nbf = args.nbf;
+      const int nbf = mats.nbf;
       for (int i = lane; i < ncd; i += 32) {
         const int c = i / g.nd, d = i - c * g.nd;
-        atomicAdd(args.J + (size_t)(fc + c) * nbf + fd + d, 2.0 * sym * Akl[i]);
+        atomicAdd(mats.J + (size_t)(fc + c) * nbf + fd + d, 2.0 * sym * Akl[i]);
       }
       for (int i = lane; i < g.nb * g.nc; i += 32) {
         const int b = i / g.nc, c = i - b * g.nc;
-        atomicAdd(args.K + (size_t)(fb + b) * nbf + fc + c, sym * Ajk[i]);
+        atomicAdd(mats.K + (size_t)(fb + b) * nbf + fc + c, sym * Ajk[i]);
       }
       for (int i = lane; i < g.nb * g.nd; i += 32) {
         const int b = i / g.nd, d = i - b * g.nd;
-        atomicAdd(args.K + (size_t)(fb + b) * nbf + fd + d, sym * Ajl[i]);
+        atomicAdd(mats.K + (size_t)(fb + b) * nbf + fd + d, sym * Ajl[i]);
       }
     } else if (args.mode == MODE_RAW) {
       if (lane == 0) {

@@ -10,8 +10,15 @@ namespace lai {
 // Thread-per-quartet kernels for the small classes (eri_small.cu).  Returns 1 if
 // the class (la,lb|lc,ld) has a specialised kernel and it was launched, 0 if the
 // class is not covered (use the generic kernel), <0 on a launch error.
+// Launch parameters of the thread-per-quartet kernels chosen by the autotuner
+// (lai_engine_autotune); 0 = the built-in heuristic.  ps = lanes per quartet
+// (primitive split, power of two), ksuper = chunks per super-chunk.
+struct LaunchTune {
+  int ps = 0;
+  int ksuper = 0;
+};
 int launch_small(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
-                 cudaStream_t stream, bool fp32, int num_sms);
+                 cudaStream_t stream, bool fp32, int num_sms, LaunchTune tune = LaunchTune{});
 bool small_class_supported(int la, int lb, int lc, int ld);
 
 // Bra-sliced kernels for the medium classes (eri_sliced.cu); same return codes.

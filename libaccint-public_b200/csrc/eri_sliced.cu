@@ -267,10 +267,11 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
   }
 
   const double sym = own ? quartet_weight(blk, p, q) : 0.0;
-  const double* __restrict__ D = args.D;
-  const int nbf = args.nbf;
-  double* __restrict__ J = args.J;
-  double* __restrict__ K = args.K;
+  const SysMats mats = sys_mats(args, blk, p);
+  const double* __restrict__ D = mats.D;
+  const int nbf = mats.nbf;
+  double* __restrict__ J = mats.J;
+  double* __restrict__ K = mats.K;
   const int arow = fa + (a < NA ? a : 0);
   // lane-complete targets
   {

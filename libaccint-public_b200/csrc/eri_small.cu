@@ -8,7 +8,7 @@ namespace lai {
 namespace small_detail {
 template <int LA, int LB, int LC, int LD>
 int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
-               cudaStream_t stream, bool fp32, int num_sms);
+               cudaStream_t stream, bool fp32, int num_sms, LaunchTune tune);
 }  // namespace small_detail
 
 #define LAI_SMALL_CLASSES(X) \
@@ -24,10 +24,10 @@ bool small_class_supported(int la, int lb, int lc, int ld) {
 }
 
 int launch_small(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
-                 cudaStream_t stream, bool fp32, int num_sms) {
+                 cudaStream_t stream, bool fp32, int num_sms, LaunchTune tune) {
   const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
 #define X(a, b, c, d) \
-  if (la == a && lb == b && lc == c && ld == d) return small_detail::launch_one<a, b, c, d>(blk, args, tab, stream, fp32, num_sms);
+  if (la == a && lb == b && lc == c && ld == d) return small_detail::launch_one<a, b, c, d>(blk, args, tab, stream, fp32, num_sms, tune);
   LAI_SMALL_CLASSES(X)
 #undef X
   return 0;

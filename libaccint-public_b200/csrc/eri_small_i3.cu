@@ -6,11 +6,11 @@ namespace lai {
 namespace small_detail {
 
 template int launch_one<1, 1, 0, 0>(const QuartetBlock&, const JKArgs&, const RysTablesView&,
-                                   cudaStream_t, bool, int);
+                                   cudaStream_t, bool, int, LaunchTune);
 template int launch_one<2, 2, 0, 0>(const QuartetBlock&, const JKArgs&, const RysTablesView&,
-                                   cudaStream_t, bool, int);
+                                   cudaStream_t, bool, int, LaunchTune);
 template int launch_one<2, 0, 1, 1>(const QuartetBlock&, const JKArgs&, const RysTablesView&,
-                                   cudaStream_t, bool, int);
+                                   cudaStream_t, bool, int, LaunchTune);
 
 }  // namespace small_detail
 }  // namespace lai

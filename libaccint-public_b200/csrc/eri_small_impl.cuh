@@ -75,101 +75,150 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   unsigned int nprim_done = 0;
   // unsplit: compile-time stride 1 keeps the bra loop warp-uniform
   const int ib0 = SPLIT ? sub : 0, ibs = SPLIT ? ps : 1;
-  for (int ib = ib0; ib < Kab; ib += ibs) {
+  // One primitive quartet: bra primitive pair (zeta, hz, P, PA, cab), ket
+  // primitive pair `cur`; accumulates into G.
+  struct BraVals {
+    R zeta, hz;
+    double Px, Py, Pz;
+    R PAx, PAy, PAz, cab;
+  };
+  auto load_bra = [&](int ib, double& qab, BraVals& v) {
     const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
-    // primitive pairs are sorted by their Schwarz bound: once the bra bound times
-    // the largest ket bound of the class drops below the cut, the rest do too
-    const double qab = __ldg(pb + PF_Q * sb);
-    if (qab * blk.ket.qprim_max < peps) break;
-    const R zeta = R(__ldg(pb + PF_ZETA * sb));
-    const R hz = R(__ldg(pb + PF_HZ * sb));
+    qab = __ldg(pb + PF_Q * sb);
+    v.zeta = R(__ldg(pb + PF_ZETA * sb));
+    v.hz = R(__ldg(pb + PF_HZ * sb));
     // P - Q is formed in FP64 on both paths: the centres are O(10) bohr, and their
     // FP32 difference would lose the digits that T = rho |PQ|^2 needs
-    const double Px = __ldg(pb + PF_PX * sb), Py = __ldg(pb + PF_PY * sb), Pz = __ldg(pb + PF_PZ * sb);
-    const R PAx = R(__ldg(pb + PF_PAX * sb)), PAy = R(__ldg(pb + PF_PAY * sb)),
-            PAz = R(__ldg(pb + PF_PAZ * sb));
-    const R cab = R(__ldg(pb + PF_C * sb));
-    const double* pk0 = blk.ket.prim + q;
+    v.Px = __ldg(pb + PF_PX * sb);
+    v.Py = __ldg(pb + PF_PY * sb);
+    v.Pz = __ldg(pb + PF_PZ * sb);
+    v.PAx = R(__ldg(pb + PF_PAX * sb));
+    v.PAy = R(__ldg(pb + PF_PAY * sb));
+    v.PAz = R(__ldg(pb + PF_PAZ * sb));
+    v.cab = R(__ldg(pb + PF_C * sb));
+  };
+  auto prim = [&](const BraVals& bv, const KetPrim& cur) {
+    const R zeta = bv.zeta, hz = bv.hz, cab = bv.cab;
+    const double Px = bv.Px, Py = bv.Py, Pz = bv.Pz;
+    const R PAx = bv.PAx, PAy = bv.PAy, PAz = bv.PAz;
+    const R eta = R(cur.eta);
+    const R he = R(cur.he);
+    const R PQx = R(Px - cur.px);
+    const R PQy = R(Py - cur.py);
+    const R PQz = R(Pz - cur.pz);
+    const R QCx = R(cur.qcx), QCy = R(cur.qcy), QCz = R(cur.qcz);
+    const R ccd = R(cur.c);
+    const R s = zeta + eta;
+    const R rs = fast_rsqrt(s);
+    const R inv = rs * rs;
+    const R rz = eta * inv, re = zeta * inv;
+    const R T = zeta * rz * (PQx * PQx + PQy * PQy + PQz * PQz);
+    const R pref = cab * ccd * rs;
+    if constexpr (NR == 1) {
+      // One root: (ss|ss) = pref F_0 and (p_i s|ss) = pref (PA_i F_0 - rz PQ_i F_1)
+      // -- the one-point Rys rule (w = F_0, u = F_1/F_0) written without its
+      // quotient.
+      R F0, F1;
+      boys01_smem<R>(T, stab, F0, F1);
+      const R pw0 = pref * F0;
+      if constexpr (LAB == 0) {
+        G[0] += pw0;
+      } else {
+        static_assert(LA == 1 && LB == 0 && LCD == 0, "one-root classes: (ss|ss), (ps|ss)");
+        const R pw1 = pref * rz * F1;
+        const R PA[3] = {PAx, PAy, PAz}, PQ[3] = {PQx, PQy, PQz};
+        sfor<0, NE>([&](auto IE) {
+          constexpr int ie = decltype(IE)::value;
+          constexpr int ce = cart_comp(LA, ie);
+          constexpr int d = comp_x(ce) ? 0 : comp_y(ce) ? 1 : 2;
+          G[ie] += PA[d] * pw0 - PQ[d] * pw1;
+        });
+      }
+      return;
+    }
+    R u[NR], w[NR];
+    rys_smem<NR, R>(T, stab, tab, u, w);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      const R ur = u[r];
+      const R b00 = R(0.5) * inv * ur;
+      const R b10 = hz - hz * rz * ur;
+      const R b01 = he - he * re * ur;
+      R I[3][LAB + 1][W];
+      const R pa[3] = {PAx - rz * ur * PQx, PAy - rz * ur * PQy, PAz - rz * ur * PQz};
+      const R qc[3] = {QCx + re * ur * PQx, QCy + re * ur * PQy, QCz + re * ur * PQz};
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        I[x][0][0] = (x == 2) ? w[r] * pref : R(1);
+#pragma unroll
+        for (int e = 0; e < LAB; ++e)
+          I[x][e + 1][0] = pa[x] * I[x][e][0] + (e ? R(e) * b10 * I[x][e > 0 ? e - 1 : 0][0] : R(0));
+#pragma unroll
+        for (int f = 0; f < LCD; ++f)
+#pragma unroll
+          for (int e = 0; e <= LAB; ++e)
+            I[x][e][f + 1] = qc[x] * I[x][e][f] +
+                             (f ? R(f) * b01 * I[x][e][f > 0 ? f - 1 : 0] : R(0)) +
+                             (e ? R(e) * b00 * I[x][e > 0 ? e - 1 : 0][f] : R(0));
+      }
+      sfor<0, NE>([&](auto IE) {
+        constexpr int ie = decltype(IE)::value;
+        // component ie of shells LA..LAB
+        constexpr int le = [] { int l = LA, r = ie; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
+        constexpr int ce = cart_comp(le, ie - ncart_before(LA, le));
+        sfor<0, NF>([&](auto JF) {
+          constexpr int jf = decltype(JF)::value;
+          constexpr int lf = [] { int l = LC, r = jf; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
+          constexpr int cf = cart_comp(lf, jf - ncart_before(LC, lf));
+          G[ie * NF + jf] += I[0][comp_x(ce)][comp_x(cf)] * I[1][comp_y(ce)][comp_y(cf)] *
+                             I[2][comp_z(ce)][comp_z(cf)];
+        });
+      });
+    }
+  };
+
+  // Loop order.  Primitive pairs are sorted by their Schwarz bound, so a loop
+  // stops once q_ab q_cd drops below the cut.  Ket data differ per lane (coalesced
+  // loads); bra data are the same for the whole warp (broadcast loads that stay in
+  // L1).  When bra and ket have the same angular momenta (typically similar
+  // primitive counts), kets go outside: each ket primitive pair is then read once
+  // per quartet instead of once per bra primitive pair (the re-reads of a warp's
+  // 32 ket rows no longer fit in L1).  Otherwise the ket side usually has more
+  // primitives (s pairs against p/d pairs) and goes inside, with its next primitive
+  // pair loaded one iteration ahead.
+  constexpr bool kKetOuter = (LAB == LCD);
+  const double* pk0 = blk.ket.prim + q;
+  if constexpr (kKetOuter) {
+    const double qab_max = ib0 < Kab ? __ldg(blk.bra.prim + (size_t)ib0 * nbra + p + PF_Q * sb) : 0.0;
     KetPrim nxt;
     load_ket_prim(pk0, sk, nxt);
     for (int ik = 0; ik < Kcd; ++ik) {
       const KetPrim cur = nxt;
-      if (qab * cur.q < peps) break;  // sorted: the rest are smaller
+      if (qab_max * cur.q < peps || ib0 >= Kab) break;
       if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
-      ++nprim_done;
-      const R eta = R(cur.eta);
-      const R he = R(cur.he);
-      const R PQx = R(Px - cur.px);
-      const R PQy = R(Py - cur.py);
-      const R PQz = R(Pz - cur.pz);
-      const R QCx = R(cur.qcx), QCy = R(cur.qcy), QCz = R(cur.qcz);
-      const R ccd = R(cur.c);
-      const R s = zeta + eta;
-      const R rs = fast_rsqrt(s);
-      const R inv = rs * rs;
-      const R rz = eta * inv, re = zeta * inv;
-      const R T = zeta * rz * (PQx * PQx + PQy * PQy + PQz * PQz);
-      const R pref = cab * ccd * rs;
-      if constexpr (NR == 1) {
-        // One root: (ss|ss) = pref F_0 and (p_i s|ss) = pref (PA_i F_0 - rz PQ_i F_1)
-        // -- the one-point Rys rule (w = F_0, u = F_1/F_0) written without its
-        // quotient.
-        R F0, F1;
-        boys01_smem<R>(T, stab, F0, F1);
-        const R pw0 = pref * F0;
-        if constexpr (LAB == 0) {
-          G[0] += pw0;
-        } else {
-          static_assert(LA == 1 && LB == 0 && LCD == 0, "one-root classes: (ss|ss), (ps|ss)");
-          const R pw1 = pref * rz * F1;
-          const R PA[3] = {PAx, PAy, PAz}, PQ[3] = {PQx, PQy, PQz};
-          sfor<0, NE>([&](auto IE) {
-            constexpr int ie = decltype(IE)::value;
-            constexpr int ce = cart_comp(LA, ie);
-            constexpr int d = comp_x(ce) ? 0 : comp_y(ce) ? 1 : 2;
-            G[ie] += PA[d] * pw0 - PQ[d] * pw1;
-          });
-        }
-        continue;
+      for (int ib = ib0; ib < Kab; ib += ibs) {
+        double qab;
+        BraVals bv;
+        load_bra(ib, qab, bv);
+        if (qab * cur.q < peps) break;
+        ++nprim_done;
+        prim(bv, cur);
       }
-      R u[NR], w[NR];
-      rys_smem<NR, R>(T, stab, tab, u, w);
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        const R ur = u[r];
-        const R b00 = R(0.5) * inv * ur;
-        const R b10 = hz - hz * rz * ur;
-        const R b01 = he - he * re * ur;
-        R I[3][LAB + 1][W];
-        const R pa[3] = {PAx - rz * ur * PQx, PAy - rz * ur * PQy, PAz - rz * ur * PQz};
-        const R qc[3] = {QCx + re * ur * PQx, QCy + re * ur * PQy, QCz + re * ur * PQz};
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-          I[x][0][0] = (x == 2) ? w[r] * pref : R(1);
-#pragma unroll
-          for (int e = 0; e < LAB; ++e)
-            I[x][e + 1][0] = pa[x] * I[x][e][0] + (e ? R(e) * b10 * I[x][e > 0 ? e - 1 : 0][0] : R(0));
-#pragma unroll
-          for (int f = 0; f < LCD; ++f)
-#pragma unroll
-            for (int e = 0; e <= LAB; ++e)
-              I[x][e][f + 1] = qc[x] * I[x][e][f] +
-                               (f ? R(f) * b01 * I[x][e][f > 0 ? f - 1 : 0] : R(0)) +
-                               (e ? R(e) * b00 * I[x][e > 0 ? e - 1 : 0][f] : R(0));
-        }
-        sfor<0, NE>([&](auto IE) {
-          constexpr int ie = decltype(IE)::value;
-          // component ie of shells LA..LAB
-          constexpr int le = [] { int l = LA, r = ie; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
-          constexpr int ce = cart_comp(le, ie - ncart_before(LA, le));
-          sfor<0, NF>([&](auto JF) {
-            constexpr int jf = decltype(JF)::value;
-            constexpr int lf = [] { int l = LC, r = jf; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
-            constexpr int cf = cart_comp(lf, jf - ncart_before(LC, lf));
-            G[ie * NF + jf] += I[0][comp_x(ce)][comp_x(cf)] * I[1][comp_y(ce)][comp_y(cf)] *
-                               I[2][comp_z(ce)][comp_z(cf)];
-          });
-        });
+    }
+  } else {
+    for (int ib = ib0; ib < Kab; ib += ibs) {
+      double qab;
+      BraVals bv;
+      load_bra(ib, qab, bv);
+      if (qab * blk.ket.qprim_max < peps) break;
+      KetPrim nxt;
+      load_ket_prim(pk0, sk, nxt);
+      for (int ik = 0; ik < Kcd; ++ik) {
+        const KetPrim cur = nxt;
+        if (qab * cur.q < peps) break;
+        if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
+        ++nprim_done;
+        prim(bv, cur);
       }
     }
   }
@@ -303,10 +352,11 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
 
   // ---- 8-fold symmetric digestion: J' += 2 s g D, K' += s g D ----
   const double sym = active ? quartet_weight(blk, p, q) : 0.0;
-  const double* __restrict__ D = args.D;
-  const int nbf = args.nbf;
-  double* __restrict__ J = args.J;
-  double* __restrict__ K = args.K;
+  const SysMats mats = sys_mats(args, blk, p);
+  const double* __restrict__ D = mats.D;
+  const int nbf = mats.nbf;
+  double* __restrict__ J = mats.J;
+  double* __restrict__ K = mats.K;
   {  // J_ij[a][b] = sum_cd V D_kl
     double Dk[NC * ND];
 #pragma unroll
@@ -415,11 +465,13 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   }
 }
 
-// (ss|ss) is latency bound with short dependent chains and fits 64 registers:
-// ask for 4 blocks (32 warps) per SM.  The other classes keep ptxas's own choice
-// (0 = no bound; an explicit 1 would let it take up to 255 registers).
+// Blocks per SM the register allocation must allow (ptxas caps registers at
+// 65536 / (256 * blocks)).  The one-root classes are latency bound with short
+// dependent chains and need the warps: (ss|ss) fits 64 registers (4 blocks, 32
+// warps), (ps|ss) 80 (3 blocks).  The other classes keep ptxas's own choice (0 =
+// no bound; an explicit 1 would let it take up to 255 registers).
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>
-__global__ void __launch_bounds__(256, (LA + LB + LC + LD == 0 ? 4 : 0))
+__global__ void __launch_bounds__(256, (LA + LB + LC + LD == 0 ? 4 : LA + LB + LC + LD == 1 ? 3 : 0))
     eri_small_kernel(QuartetBlock blk, JKArgs args, RysTablesView tab, int kSuper, int ps) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -467,7 +519,7 @@ namespace small_detail {
 
 template <int LA, int LB, int LC, int LD>
 int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
-               cudaStream_t stream, bool fp32, int num_sms) {
+               cudaStream_t stream, bool fp32, int num_sms, LaunchTune tune) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   const int threads = 256;
   const size_t smem = fp32 ? table_bytes<NR, float>() : table_bytes<NR, double>();
@@ -478,6 +530,7 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
   const int Kab = blk.bra.Ka * blk.bra.Kb;
   int ps = 1;
   while (ps < 32 && ps < Kab && nq * ps < (int64_t)num_sms * 1024) ps <<= 1;
+  if (tune.ps > 0) ps = tune.ps;
   const int64_t nchunks = (nq + 32 / ps - 1) / (32 / ps);
   // separate instantiations keep the unsplit kernel's register allocation
   // independent of the split one
@@ -502,7 +555,8 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
   // chunks per super-chunk: long runs (one bra search each) when the launch has
   // plenty of work, short ones when it would otherwise leave warps idle
   const int64_t warps_total = (int64_t)grid * (threads / 32);
-  const int ksuper = (int)std::max<int64_t>(1, std::min<int64_t>(16, nchunks / (8 * warps_total)));
+  const int ksuper = tune.ksuper > 0 ? tune.ksuper
+                                     : (int)std::max<int64_t>(1, std::min<int64_t>(16, nchunks / (8 * warps_total)));
   kern<<<grid, threads, smem, stream>>>(blk, args, tab, ksuper, ps);
   return cudaGetLastError() == cudaSuccess ? 1 : -3;
 }

@@ -42,6 +42,7 @@ int lai_engine_natom(lai_engine* engine) {
 }
 
 int lai_jk_gradient_device(lai_engine* engine, const double* d_D, double* d_grad, void* stream) {
+  if (engine && engine->nsys > 1) return fail(LAI_ENOTSUP, "lai_jk_gradient: not available for a batched engine");
   if (!engine || !d_D || !d_grad) return fail(LAI_EINVAL, "lai_jk_gradient_device: null argument");
   LAI_CUDA_TRY(cudaSetDevice(engine->device));
   if (int rc = ensure_atoms(engine)) return rc;

@@ -31,6 +31,7 @@ namespace lai {
 int engine_device(const lai_engine* E);
 int engine_num_sms(const lai_engine* E);
 int engine_nbf(const lai_engine* E);
+int engine_nsys(const lai_engine* E);
 double engine_prim_eps(const lai_engine* E);
 RysTablesView engine_tables(const lai_engine* E);
 int engine_block_count(const lai_engine* E);
@@ -69,6 +70,8 @@ int err(int code, const char* msg) {
 extern "C" int lai_jk_build_noalloc(lai_engine* engine, const double* d_D, double* d_J,
                                     double* d_K, void* stream) {
   if (!engine || !d_D || !d_J || !d_K) return err(LAI_EINVAL, "lai_jk_build_noalloc: null argument");
+  if (lai::engine_nsys(engine) > 1)
+    return err(LAI_ENOTSUP, "lai_jk_build_noalloc: not available for a batched engine");
   const int nbf = lai::engine_nbf(engine);
   if (nbf > kMaxNbf)
     return err(LAI_EINVAL, "lai_jk_build_noalloc: nbf exceeds LAI_NOALLOC_MAX_NBF (512); "

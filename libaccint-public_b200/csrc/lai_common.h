@@ -53,6 +53,7 @@ struct PairClassDev {
   const double* AB;    // [3 * npairs] A - B, SoA
   const double* prim;  // [PF_COUNT * Ka*Kb * npairs]
   double qprim_max;    // largest PF_Q of the class
+  const int* sys;      // [npairs] system of each pair in a batched engine, else nullptr
 };
 
 // One launch: the canonical quartets (p, q) with p a pair of class `bra` and q a

@@ -251,6 +251,7 @@ extern "C" {
 
 int lai_eri_quartets(lai_engine* engine, const int32_t* quartets, int64_t n, double* out,
                      size_t out_capacity, lai_quartet_meta* meta) {
+  if (engine && engine->nsys > 1) return fail(LAI_ENOTSUP, "lai_eri_quartets: not available for a batched engine");
   if (!engine || n < 0 || (n > 0 && (!quartets || !out || !meta)))
     return fail(LAI_EINVAL, "lai_eri_quartets: null argument");
   if (n == 0) return LAI_OK;
@@ -306,6 +307,7 @@ int lai_eri_quartets(lai_engine* engine, const int32_t* quartets, int64_t n, dou
 int lai_jk_accumulate_quartets_device(lai_engine* engine, const int32_t* quartets, int64_t n,
                                       const double* d_D, double* d_J, double* d_K, void* stream,
                                       int canonical_symmetry) {
+  if (engine && engine->nsys > 1) return fail(LAI_ENOTSUP, "lai_jk_accumulate_quartets: not available for a batched engine");
   if (!engine || n < 0 || (n > 0 && !quartets) || !d_D || !d_J || !d_K)
     return fail(LAI_EINVAL, "lai_jk_accumulate_quartets: null argument");
   if (n == 0) return LAI_OK;
@@ -319,6 +321,7 @@ int lai_jk_accumulate_quartets_device(lai_engine* engine, const int32_t* quartet
   if (canonical_symmetry) {
     const size_t bytes = sizeof(double) * (size_t)nbf * nbf;
     if (engine->d_Jp.bytes < bytes) {
+      engine->release_graph();
       LAI_CUDA_TRY(engine->d_Jp.alloc(bytes));
       LAI_CUDA_TRY(engine->d_Kp.alloc(bytes));
     }
@@ -390,6 +393,7 @@ int lai_jk_accumulate_quartets(lai_engine* engine, const int32_t* quartets, int6
 int lai_jk_accumulate_eri_batch_device(lai_engine* engine, const double* d_eri, const lai_quartet_meta* meta,
                                        int64_t n, const double* d_D, double* d_J, double* d_K,
                                        void* stream) {
+  if (engine && engine->nsys > 1) return fail(LAI_ENOTSUP, "lai_jk_accumulate_eri_batch_device: not available for a batched engine");
   if (!engine || n < 0 || (n > 0 && (!d_eri || !meta)) || !d_D || !d_J || !d_K)
     return fail(LAI_EINVAL, "lai_jk_accumulate_eri_batch_device: null argument");
   if (n == 0) return LAI_OK;

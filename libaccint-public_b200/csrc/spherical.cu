@@ -29,6 +29,7 @@
 namespace lai {
 int engine_device(const lai_engine* E);
 const lai_basis* engine_basis(const lai_engine* E);
+int engine_nsys(const lai_engine* E);
 void engine_set_error(const char* msg);
 }  // namespace lai
 
@@ -332,6 +333,7 @@ int lai_sph_to_cart_density(const lai_basis* basis, const double* D_sph, double*
 
 int lai_cart_to_sph_2d_device(lai_engine* engine, const double* d_M_cart, double* d_M_sph, void* stream) {
   if (!engine || !d_M_cart || !d_M_sph) return err(LAI_EINVAL, "lai_cart_to_sph_2d_device: null argument");
+  if (lai::engine_nsys(engine) > 1) return err(LAI_ENOTSUP, "lai_cart_to_sph_2d_device: not available for a batched engine");
   const int dev = lai::engine_device(engine);
   if (cudaSetDevice(dev) != cudaSuccess) return err(LAI_ECUDA, "lai_cart_to_sph_2d_device: cudaSetDevice");
   DevMap m;
@@ -347,6 +349,7 @@ int lai_cart_to_sph_2d_device(lai_engine* engine, const double* d_M_cart, double
 int lai_sph_to_cart_density_device(lai_engine* engine, const double* d_D_sph, double* d_D_cart,
                                    void* stream) {
   if (!engine || !d_D_sph || !d_D_cart) return err(LAI_EINVAL, "lai_sph_to_cart_density_device: null argument");
+  if (lai::engine_nsys(engine) > 1) return err(LAI_ENOTSUP, "lai_sph_to_cart_density_device: not available for a batched engine");
   const int dev = lai::engine_device(engine);
   if (cudaSetDevice(dev) != cudaSuccess) return err(LAI_ECUDA, "lai_sph_to_cart_density_device: cudaSetDevice");
   DevMap m;

@@ -109,13 +109,14 @@ class Engine:
         return Q
 
     @staticmethod
-    def _opts(fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False):
+    def _opts(fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False, graph=False):
         opts = _lib.JKOpts()
         _lib.lib().lai_jk_opts_default(ctypes.byref(opts))
         opts.fp32_cut = fp32_cut
         opts.check_symmetric = int(check_symmetric)
         opts.shard_index, opts.shard_count = shard
         opts.profile = int(profile)
+        opts.graph = int(graph)
         return opts
 
     def jk(self, D, fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False, out=None):
@@ -145,10 +146,11 @@ class Engine:
         J, K, rep = self.jk(Dc, fp32_cut=fp32_cut)
         return self.basis.cart_to_sph(J), self.basis.cart_to_sph(K), rep
 
-    def jk_device(self, d_D, d_J, d_K, stream=0, fp32_cut=0.0, shard=(0, 1), profile=False):
-        """Device-pointer variant (integers from torch.Tensor.data_ptr())."""
+    def jk_device(self, d_D, d_J, d_K, stream=0, fp32_cut=0.0, shard=(0, 1), profile=False, graph=False):
+        """Device-pointer variant (integers from torch.Tensor.data_ptr()).  graph=True
+        captures the build as a CUDA graph on the first call and replays it after."""
         L = _lib.lib()
-        opts = self._opts(fp32_cut, False, shard, profile)
+        opts = self._opts(fp32_cut, False, shard, profile, graph)
         rep = _lib.JKReport()
         _lib.check(L.lai_jk_build_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
                                          ctypes.c_void_p(d_K), ctypes.c_void_p(stream),
@@ -226,6 +228,15 @@ class Engine:
                                                          J.ctypes.data, K.ctypes.data,
                                                          int(bool(canonical_symmetry))))
 
+    def autotune(self, d_D, stream=0):
+        """Times each class launch under a few launch configurations on the device
+        density d_D and keeps the fastest; returns (ms_before, ms_after)."""
+        a = ctypes.c_double()
+        b = ctypes.c_double()
+        _lib.check(_lib.lib().lai_engine_autotune(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(stream),
+                                                  ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def natom(self):
         n = _lib.lib().lai_engine_natom(self._h)
         if n < 0:
@@ -270,6 +281,58 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+class BatchedEngine(Engine):
+    """Many independent systems (a list of BasisSet) in one engine: every
+    shell-quartet class of all systems runs as one persistent launch.  D, J and K
+    are lists of per-system matrices on the host side, packed on the device
+    (``layout()`` gives the element offsets)."""
+
+    def __init__(self, bases, threshold=1e-12, device=0, prim_threshold=None):
+        self.bases = list(bases)
+        self.basis = None
+        self.threshold = threshold
+        L = _lib.lib()
+        opts = _lib.EngineOpts()
+        L.lai_engine_opts_default(ctypes.byref(opts))
+        opts.schwarz_threshold = threshold
+        opts.device = device
+        if prim_threshold is not None:
+            opts.prim_threshold = prim_threshold
+        handles = (ctypes.c_void_p * len(self.bases))(*[b.handle() for b in self.bases])
+        h = ctypes.c_void_p()
+        _lib.check(L.lai_engine_create_batched(len(self.bases), handles, ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+
+    def layout(self):
+        n = len(self.bases)
+        off = np.zeros(n + 1, dtype=np.int64)
+        nbf = np.zeros(n, dtype=np.int32)
+        _lib.check(_lib.lib().lai_engine_batch_layout(self._h, None, off.ctypes.data, nbf.ctypes.data))
+        return off, nbf
+
+    def pack(self, mats):
+        off, nbf = self.layout()
+        out = np.empty(int(off[-1]))
+        for s, M in enumerate(mats):
+            out[off[s]:off[s + 1]] = np.ascontiguousarray(M, dtype=np.float64).reshape(-1)
+        return out
+
+    def unpack(self, packed):
+        off, nbf = self.layout()
+        return [packed[off[s]:off[s + 1]].reshape(nbf[s], nbf[s]) for s in range(len(nbf))]
+
+    def jk(self, Ds, fp32_cut=0.0, profile=False):
+        """([J_s], [K_s], report) for the per-system densities Ds."""
+        D = self.pack(Ds)
+        J = np.empty_like(D)
+        K = np.empty_like(D)
+        opts = self._opts(fp32_cut, False, (0, 1), profile)
+        rep = _lib.JKReport()
+        _lib.check(_lib.lib().lai_jk_build_batched(self._h, D.ctypes.data, J.ctypes.data, K.ctypes.data,
+                                                   ctypes.byref(opts), ctypes.byref(rep)))
+        return self.unpack(J), self.unpack(K), rep
 
 
 def probe_fp64_peak(device=0):
