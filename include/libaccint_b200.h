@@ -130,6 +130,11 @@ typedef struct {
                           the FP32 cut derived from max|D| at capture time.     */
 } lai_jk_opts;
 LAI_API void lai_jk_opts_default(lai_jk_opts* opts);
+/* The slice [lo, hi) of a block of `total` quartets that shard `index` of `count`
+ * computes (contiguous, sizes differ by at most one; the shards tile [0, total)).
+ * Host-only arithmetic, no device needed.  The multi-GPU driver calls the build
+ * with shard_index = rank, shard_count = world size and sums J and K over ranks. */
+LAI_API int lai_shard_range(int64_t total, int index, int count, int64_t* lo, int64_t* hi);
 
 typedef struct {
   int64_t quartets_fp64;   /* canonical shell quartets computed in FP64       */
@@ -301,6 +306,11 @@ LAI_API int64_t lai_engine_quartet_count(lai_engine* engine);
  * heuristic and with the chosen configurations.  Synchronizes `stream`. */
 LAI_API int lai_engine_autotune(lai_engine* engine, const double* d_D, void* stream, double* ms_before,
                                 double* ms_after);
+/* The launch table: per class-pair block, 10 ints: la, lb, lc, ld, bra and ket
+ * primitive pairs per shell pair, quartets (capped at INT32_MAX), tuned lanes per
+ * quartet and chunks per super-chunk (0 = heuristic), quartets / 1000.  Returns
+ * the block count; rows may be NULL to query it. */
+LAI_API int lai_engine_tune_table(lai_engine* engine, int capacity, int* rows);
 /* FP64 FMA throughput of the device measured by a register-resident FMA loop
  * (TFLOP/s, 2 FLOP per FMA): the speed-of-light denominator of the FP64 path. */
 LAI_API int lai_probe_fp64_peak(int device, double* tflops);

@@ -27,7 +27,7 @@ EXPORTED = [
     "lai_jk_accumulate_eri_batch_device",
     "lai_engine_natom", "lai_jk_gradient", "lai_jk_gradient_device",
     "lai_engine_create_batched", "lai_engine_batch_layout", "lai_jk_build_batched",
-    "lai_engine_autotune",
+    "lai_engine_autotune", "lai_shard_range", "lai_engine_tune_table",
 ]
 
 
@@ -112,6 +112,8 @@ def lib():
         "lai_engine_batch_layout": (I, [P, P, P, P]),
         "lai_jk_build_batched": (I, [P, P, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKReport)]),
         "lai_engine_autotune": (I, [P, P, P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+        "lai_shard_range": (I, [ctypes.c_int64, I, I, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+        "lai_engine_tune_table": (I, [P, I, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

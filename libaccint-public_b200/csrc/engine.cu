@@ -692,8 +692,8 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
         if (part == 1) q.qbegin = bp.d_qb32.as<int>();  // the FP64 part keeps the block's ket starts
       }
       // this shard's contiguous slice of the part
-      const int64_t lo = total * o.shard_index / o.shard_count;
-      const int64_t hi = total * (o.shard_index + 1) / o.shard_count;
+      int64_t lo = 0, hi = 0;
+      lai_shard_range(total, o.shard_index, o.shard_count, &lo, &hi);
       if (hi <= lo) continue;
       q.t_begin = lo;
       q.total = hi;
@@ -765,6 +765,15 @@ __global__ void fp64_fma_probe(double* out, int iters) {
 }  // namespace lai
 
 extern "C" {
+
+int lai_shard_range(int64_t total, int index, int count, int64_t* lo, int64_t* hi) {
+  if (count < 1 || index < 0 || index >= count || total < 0 || !lo || !hi)
+    return fail(LAI_EINVAL, "lai_shard_range: bad arguments");
+  // 128-bit products: total * count may exceed 63 bits for huge blocks
+  *lo = (int64_t)((__int128)total * index / count);
+  *hi = (int64_t)((__int128)total * (index + 1) / count);
+  return LAI_OK;
+}
 
 void lai_engine_opts_default(lai_engine_opts* opts) {
   if (!opts) return;
@@ -1218,6 +1227,24 @@ int lai_engine_autotune(lai_engine* engine, const double* d_D, void* stream, dou
   if (ms_before) *ms_before = before;
   if (ms_after) *ms_after = after;
   return LAI_OK;
+}
+
+int lai_engine_tune_table(lai_engine* engine, int capacity, int* rows) {
+  if (!engine) return fail(LAI_EINVAL, "lai_engine_tune_table: null engine");
+  const int n = (int)engine->blocks.size();
+  if (!rows || capacity < n) return n;
+  for (int b = 0; b < n; ++b) {
+    const auto& bp = *engine->blocks[b];
+    const auto& ca = *engine->classes[bp.bra];
+    const auto& cb = *engine->classes[bp.ket];
+    int* r = rows + 10 * b;
+    r[0] = ca.la; r[1] = ca.lb; r[2] = cb.la; r[3] = cb.lb;
+    r[4] = ca.Ka * ca.Kb; r[5] = cb.Ka * cb.Kb;
+    r[6] = (int)std::min<int64_t>(bp.total, INT32_MAX);
+    r[7] = bp.tune.ps; r[8] = bp.tune.ksuper;
+    r[9] = (int)std::min<int64_t>(bp.total / 1000, INT32_MAX);
+  }
+  return n;
 }
 
 int lai_probe_fp64_peak(int device, double* tflops) {

@@ -237,6 +237,14 @@ class Engine:
                                                   ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def tune_table(self):
+        """Per class-pair block: la, lb, lc, ld, Kab, Kcd, quartets, ps, ksuper, quartets/1000."""
+        L = _lib.lib()
+        n = L.lai_engine_tune_table(self._h, 0, None)
+        rows = np.zeros((max(n, 1), 10), dtype=np.int32)
+        L.lai_engine_tune_table(self._h, n, rows.ctypes.data)
+        return rows[:n]
+
     def natom(self):
         n = _lib.lib().lai_engine_natom(self._h)
         if n < 0:

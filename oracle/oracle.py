@@ -43,6 +43,7 @@ def restatement():
         L.orc_eri_quartet.argtypes = [_P, _P, _P, _P, _P, _P]
         L.orc_basis_quartet.argtypes = [_I, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P]
         L.orc_basis_quartets.argtypes = [_I, _P, _P, _P, _P, _P, _L, _P, _P]
+        L.orc_jk_list.argtypes = [_I, _P, _P, _P, _P, _P, _P, _L, _P, _P, _P]
         L.orc_schwarz.argtypes = [_I, _P, _P, _P, _P, _P, _P]
         L.orc_jk_sym.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _D]
         L.orc_jk_sym.restype = ctypes.c_long
@@ -140,6 +141,16 @@ def orc_quartet(basis, i, j, k, m):
                              exps.ctypes.data, coefs.ctypes.data, i, j, k, m, out.ctypes.data)
     assert rc == 0
     return out.reshape(nf)
+
+
+def orc_jk_list(basis, D, quartets, J, K):
+    """Adds the 8-fold symmetric J/K contributions of listed canonical quartets."""
+    O = restatement()
+    l, nprim, centers, exps, coefs = normalized_arrays(basis)
+    q = np.ascontiguousarray(quartets, dtype=np.int32)
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    O.orc_jk_list(len(l), l.ctypes.data, nprim.ctypes.data, centers.ctypes.data, exps.ctypes.data,
+                  coefs.ctypes.data, D.ctypes.data, len(q), q.ctypes.data, J.ctypes.data, K.ctypes.data)
 
 
 def orc_quartets(basis, quartets):

@@ -363,6 +363,26 @@ int orc_basis_quartet(int n, const int *l, const int *nprim, const double *ctr, 
     return rc;
 }
 
+static void scatter_sym(const basis_t *b, const int *l, long nbf, int i, int j, int k, int m,
+                        const double *g, const double *D, double *J, double *K);
+
+/* J/K contributions of listed canonical quartets (shell indices q[4t..4t+3],
+   i >= j, k >= l, ij >= kl in the canonical loop's sense), ADDED to J and K. */
+void orc_jk_list(int n, const int *l, const int *nprim, const double *ctr, const double *exps,
+                 const double *coefs, const double *D, long nq, const int *q, double *J, double *K) {
+    basis_t b;
+    basis_init(&b, n, l, nprim, ctr, exps, coefs);
+    const long nbf = b.foff[n];
+    double *g = malloc(sizeof(double) * 28 * 28 * 28 * 28);
+    for (long t = 0; t < nq; ++t) {
+        const int *x = q + 4 * t;
+        quartet(&b, x[0], x[1], x[2], x[3], g);
+        scatter_sym(&b, l, nbf, x[0], x[1], x[2], x[3], g, D, J, K);
+    }
+    free(g);
+    basis_free(&b);
+}
+
 /* Many contracted quartets (shell indices q[4t..4t+3]), blocks concatenated in
    order into out (each [a][b][c][d]); OpenMP over quartets.  Returns 0. */
 int orc_basis_quartets(int n, const int *l, const int *nprim, const double *ctr, const double *exps,
@@ -406,6 +426,53 @@ int orc_schwarz(int n, const int *l, const int *nprim, const double *ctr, const 
     return 0;
 }
 
+/* 8-fold symmetric scatter of one canonical quartet's block g into J, K
+   (fock_builder.cpp:123-222 accumulate_symmetric). */
+static void scatter_sym(const basis_t *b, const int *l, long nbf, int i, int j, int k, int m,
+                        const double *g, const double *D, double *J, double *K) {
+    const int ij = (i == j), kl = (k == m), bk = (i == k && j == m);
+    const int na = ncart(l[i]), nb = ncart(l[j]), nc = ncart(l[k]), nd = ncart(l[m]);
+    long o = 0;
+    for (int a = 0; a < na; ++a)
+        for (int bb = 0; bb < nb; ++bb)
+            for (int c = 0; c < nc; ++c)
+                for (int d = 0; d < nd; ++d, ++o) {
+                    const long mu = b->foff[i] + a, nu = b->foff[j] + bb;
+                    const long la = b->foff[k] + c, si = b->foff[m] + d;
+                    const double v = g[o];
+                    J[mu * nbf + nu] += v * D[la * nbf + si];
+                    K[mu * nbf + la] += v * D[nu * nbf + si];
+                    if (!kl) {
+                        J[mu * nbf + nu] += v * D[si * nbf + la];
+                        K[mu * nbf + si] += v * D[nu * nbf + la];
+                    }
+                    if (!ij) {
+                        J[nu * nbf + mu] += v * D[la * nbf + si];
+                        K[nu * nbf + la] += v * D[mu * nbf + si];
+                    }
+                    if (!ij && !kl) {
+                        J[nu * nbf + mu] += v * D[si * nbf + la];
+                        K[nu * nbf + si] += v * D[mu * nbf + la];
+                    }
+                    if (!bk) {
+                        J[la * nbf + si] += v * D[mu * nbf + nu];
+                        K[la * nbf + mu] += v * D[nu * nbf + si];
+                        if (!ij) {
+                            J[la * nbf + si] += v * D[nu * nbf + mu];
+                            K[la * nbf + nu] += v * D[mu * nbf + si];
+                        }
+                        if (!kl) {
+                            J[si * nbf + la] += v * D[mu * nbf + nu];
+                            K[si * nbf + mu] += v * D[nu * nbf + la];
+                        }
+                        if (!ij && !kl) {
+                            J[si * nbf + la] += v * D[nu * nbf + mu];
+                            K[si * nbf + nu] += v * D[mu * nbf + la];
+                        }
+                    }
+                }
+}
+
 /* Canonical screened loop + 8-fold symmetric scatter (serial).  D symmetric,
    row-major nbf x nbf; J and K are overwritten.  Returns the number of
    canonical quartets computed. */
@@ -427,47 +494,7 @@ long orc_jk_sym(int n, const int *l, const int *nprim, const double *ctr, const 
                     if (Q[i * n + j] * Q[k * n + m] < thr) continue;
                     quartet(&b, i, j, k, m, g);
                     ++count;
-                    const int ij = (i == j), kl = (k == m), bk = (i == k && j == m);
-                    const int na = ncart(l[i]), nb = ncart(l[j]), nc = ncart(l[k]), nd = ncart(l[m]);
-                    long o = 0;
-                    for (int a = 0; a < na; ++a)
-                        for (int bb = 0; bb < nb; ++bb)
-                            for (int c = 0; c < nc; ++c)
-                                for (int d = 0; d < nd; ++d, ++o) {
-                                    const long mu = b.foff[i] + a, nu = b.foff[j] + bb;
-                                    const long la = b.foff[k] + c, si = b.foff[m] + d;
-                                    const double v = g[o];
-                                    J[mu * nbf + nu] += v * D[la * nbf + si];
-                                    K[mu * nbf + la] += v * D[nu * nbf + si];
-                                    if (!kl) {
-                                        J[mu * nbf + nu] += v * D[si * nbf + la];
-                                        K[mu * nbf + si] += v * D[nu * nbf + la];
-                                    }
-                                    if (!ij) {
-                                        J[nu * nbf + mu] += v * D[la * nbf + si];
-                                        K[nu * nbf + la] += v * D[mu * nbf + si];
-                                    }
-                                    if (!ij && !kl) {
-                                        J[nu * nbf + mu] += v * D[si * nbf + la];
-                                        K[nu * nbf + si] += v * D[mu * nbf + la];
-                                    }
-                                    if (!bk) {
-                                        J[la * nbf + si] += v * D[mu * nbf + nu];
-                                        K[la * nbf + mu] += v * D[nu * nbf + si];
-                                        if (!ij) {
-                                            J[la * nbf + si] += v * D[nu * nbf + mu];
-                                            K[la * nbf + nu] += v * D[mu * nbf + si];
-                                        }
-                                        if (!kl) {
-                                            J[si * nbf + la] += v * D[mu * nbf + nu];
-                                            K[si * nbf + mu] += v * D[nu * nbf + la];
-                                        }
-                                        if (!ij && !kl) {
-                                            J[si * nbf + la] += v * D[nu * nbf + mu];
-                                            K[si * nbf + nu] += v * D[mu * nbf + la];
-                                        }
-                                    }
-                                }
+                    scatter_sym(&b, l, nbf, i, j, k, m, g, D, J, K);
                 }
     free(g);
     free(Q);
