@@ -36,6 +36,14 @@ WORKLOAD = "h2o64_ccpvdz"
 METRIC = "jk_quartets_per_s"
 UNIT = "quartets/s"
 
+SYSTEMS = {
+    "h2o64_ccpvdz": "(H2O)64 4x4x4 grid, cc-pVDZ (Cartesian)",
+    "h2o16_ccpvdz": "(H2O)16 2x2x4 grid, cc-pVDZ (Cartesian)",
+    "h2o8_sto3g": "(H2O)8 2x2x2 grid, built-in STO-3G",
+    "c12h26_ccpvtz": "all-trans C12H26, cc-pVTZ (Cartesian, s..f)",
+    "c12h26_ccpvqz": "all-trans C12H26, cc-pVQZ (Cartesian, s..g)",
+}
+
 # DRAM bytes (read + write) per launch of a class kernel, averaged over the launches of
 # one timed step in a one-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum);
 # the capture and its command are summarised under profiles/.
@@ -445,7 +453,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "system": "(H2O)64 4x4x4 grid, cc-pVDZ (Cartesian)",
+            "config": {"workload": args.workload, "system": SYSTEMS.get(args.workload, args.workload),
                        "nbf": n, "shells": w.basis.n_shells, "quartets": total_q, "schwarz": w.thr,
                        "nocc": w.nocc, "parallelism": f"quartet shards x{ws}" + (" + NCCL all-reduce" if ws > 1 else ""),
                        "l2": "flushed (256 MB write) between timed steps"},

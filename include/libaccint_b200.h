@@ -163,8 +163,7 @@ LAI_API int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d
  * start-up.  Same result as lai_jk_build_device(); the two nbf x nbf
  * accumulators live in a fixed 4 MiB array of the library's device image
  * (held on every GPU that loads the library until exit), hence
- * nbf <= LAI_NOALLOC_MAX_NBF, else LAI_EINVAL; bases with a class whose
- * integral block needs global scratch give LAI_ENOTSUP.  All calls share the
+ * nbf <= LAI_NOALLOC_MAX_NBF, else LAI_EINVAL.  All calls share the
  * array: calls whose device work overlaps race.  The first call on a device
  * looks up the array's address -- make it before any stream capture.
  * Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream). */
@@ -278,6 +277,31 @@ LAI_API int lai_cart_to_sph_2d_device(lai_engine* engine, const double* d_M_cart
                                       void* stream);
 LAI_API int lai_sph_to_cart_density_device(lai_engine* engine, const double* d_D_sph, double* d_D_cart,
                                            void* stream);
+
+/* ---------------------------------------------------------------------------
+ * One-electron integrals over the engine's basis, full nbf x nbf row-major
+ * (symmetric), same normalization and Cartesian order as J/K:
+ *   LAI_OP_OVERLAP  S_ab = <a|b>
+ *   LAI_OP_KINETIC  T_ab = <a|-1/2 nabla^2|b>
+ *   LAI_OP_NUCLEAR  V_ab = -sum_C q_C <a|1/|r-C||b>   (point charges; atomic
+ *                   numbers for the nuclei)
+ *   LAI_OP_HCORE    T + V in one pass
+ * Replaces Engine::compute_1e(OneElectronOperator, result) / compute_overlap_matrix /
+ * compute_kinetic_matrix / compute_nuclear_matrix (include/libaccint/engine/
+ * engine.hpp:166-201, 831-900; kernels src/host/kernels/{overlap,kinetic,nuclear}
+ * _kernel.cpp).  charge_xyz [ncharge][3] (Bohr) and charge_q [ncharge] are host
+ * arrays (NULL with ncharge = 0 for S and T).  Not available for batched engines.
+ * ------------------------------------------------------------------------- */
+#define LAI_OP_OVERLAP 0
+#define LAI_OP_KINETIC 1
+#define LAI_OP_NUCLEAR 2
+#define LAI_OP_HCORE 3
+LAI_API int lai_one_electron(lai_engine* engine, int op, int ncharge, const double* charge_xyz,
+                             const double* charge_q, double* out);
+/* Device output (nbf x nbf), asynchronous on stream (charges are staged through
+ * the engine before the call returns). */
+LAI_API int lai_one_electron_device(lai_engine* engine, int op, int ncharge, const double* charge_xyz,
+                                    const double* charge_q, double* d_out, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Measurement helpers (no counterpart in the reference, which has no device

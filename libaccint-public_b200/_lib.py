@@ -28,7 +28,10 @@ EXPORTED = [
     "lai_engine_natom", "lai_jk_gradient", "lai_jk_gradient_device",
     "lai_engine_create_batched", "lai_engine_batch_layout", "lai_jk_build_batched",
     "lai_engine_autotune", "lai_shard_range", "lai_engine_tune_table",
+    "lai_one_electron", "lai_one_electron_device",
 ]
+
+LAI_OP_OVERLAP, LAI_OP_KINETIC, LAI_OP_NUCLEAR, LAI_OP_HCORE = 0, 1, 2, 3
 
 
 class LibAccIntError(RuntimeError):
@@ -114,6 +117,8 @@ def lib():
         "lai_engine_autotune": (I, [P, P, P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
         "lai_shard_range": (I, [ctypes.c_int64, I, I, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
         "lai_engine_tune_table": (I, [P, I, P]),
+        "lai_one_electron": (I, [P, I, I, P, P, P]),
+        "lai_one_electron_device": (I, [P, I, I, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -41,6 +41,37 @@ def cart_to_sph_matrix(l):
     return C
 
 
+class Atom:
+    """Atomic number and position (Bohr): data::Atom of the reference
+    (include/libaccint/data/builtin_basis.hpp:17)."""
+    __slots__ = ("atomic_number", "position")
+
+    def __init__(self, atomic_number, position):
+        self.atomic_number = int(atomic_number)
+        self.position = np.asarray(position, dtype=np.float64).reshape(3)
+
+
+def point_charges(atoms):
+    """(xyz [n][3], q [n]) from a list of Atom or (Z, (x, y, z)) pairs, or from an
+    object with x, y, z, charge sequences (PointChargeParams of the reference,
+    include/libaccint/operators/operator_types.hpp:50-60)."""
+    if hasattr(atoms, "charge"):
+        xyz = np.stack([np.asarray(atoms.x, dtype=np.float64), np.asarray(atoms.y, dtype=np.float64),
+                        np.asarray(atoms.z, dtype=np.float64)], axis=1)
+        return np.ascontiguousarray(xyz), np.ascontiguousarray(atoms.charge, dtype=np.float64)
+    xyz, q = [], []
+    for a in atoms:
+        if isinstance(a, Atom):
+            q.append(float(a.atomic_number))
+            xyz.append(a.position)
+        else:
+            z, r = a
+            q.append(float(z))
+            xyz.append(np.asarray(r, dtype=np.float64).reshape(3))
+    return (np.ascontiguousarray(np.array(xyz, dtype=np.float64).reshape(-1, 3)),
+            np.ascontiguousarray(q, dtype=np.float64))
+
+
 class Shell:
     __slots__ = ("l", "center", "exps", "coefs", "atom")
 
@@ -63,6 +94,7 @@ class BasisSet:
         self.shells = list(shells)
         self.prenormalized = prenormalized
         self._handle = None
+        self.atoms = None   # [Atom] when built by from_atoms
 
     @classmethod
     def from_atoms(cls, Z, xyz, name):
@@ -75,7 +107,9 @@ class BasisSet:
                 raise KeyError(f"element Z={z} not in basis {name}")
             for l, e, c in data[sym]:
                 shells.append(Shell(l, r, e, c, a))
-        return cls(shells)
+        b = cls(shells)
+        b.atoms = [Atom(z, r) for z, r in zip(Z, xyz)]
+        return b
 
     # --- flat arrays (the C-ABI layout) ---
     def arrays(self):

@@ -317,6 +317,12 @@ int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs&
                                            cudaGetErrorString(cudaGetLastError()));
     return LAI_OK;
   }
+  {
+    const int rc = lai::launch_tiled(blk, args, E->tab, E->stream, E->num_sms);
+    if (rc == 0) return LAI_OK;
+    if (rc < -1) return fail(LAI_ECUDA, std::string("tiled launch failed: ") +
+                                            cudaGetErrorString(cudaGetLastError()));
+  }
   const size_t need = lai::generic_global_scratch_doubles(la, lb, lc, ld, E->num_sms);
   if (int rc = ensure_scratch(E, need)) return rc;
   const int rc = lai::launch_generic(blk, args, E->tab, E->stream, E->d_scratch.as<double>(),
@@ -475,6 +481,11 @@ int sort_and_screen(lai_engine* E) {
     c.batched = batched;
     if (int rc = upload_class(c)) return rc;
     if (batched) LAI_CUDA_TRY(upload(c.d_sys, c.sys));
+    {  // FP32 copy of the primitive-pair table for the FP32 kernels
+      std::vector<float> pf(c.prim.size());
+      for (size_t i = 0; i < pf.size(); ++i) pf[i] = (float)c.prim[i];
+      LAI_CUDA_TRY(upload(c.d_primf, pf));
+    }
   }
   // quartet blocks
   const int nc = (int)E->classes.size();

@@ -86,7 +86,7 @@ struct PairClassHost {
   std::vector<double> prim;        // SoA [PF_COUNT][Kab][n]
   int n() const { return (int)sa.size(); }
   // device copies
-  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_prim, d_sys;
+  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_prim, d_sys, d_primf;
   bool batched = false;             // d_sys is set (more than one system)
   lai::PairClassDev view() const {
     lai::PairClassDev v;
@@ -96,6 +96,7 @@ struct PairClassHost {
     v.Q = d_Q.as<double>(); v.AB = d_AB.as<double>(); v.prim = d_prim.as<double>();
     v.qprim_max = qprim_max;
     v.sys = batched ? d_sys.as<int>() : nullptr;
+    v.primf = d_primf.as<float>();
     return v;
   }
 };
@@ -149,6 +150,11 @@ struct lai_engine {
   lai::host::DevBuf d_absmax;
   lai::host::DevBuf d_shell_atom;  // [nshell] atom of each shell (gradients)
   int natom = -1;
+  // one-electron integrals: shell table, primitives and shell pairs grouped by
+  // (la, lb) class (built on first use; one_electron.cu)
+  lai::host::DevBuf d_1e_shell, d_1e_exp, d_1e_coef, d_1e_pairs, d_1e_charges;
+  std::vector<int> one_e_class;    // per class: la, lb, first pair, pair count
+  size_t charges_cap = 0;
   // CUDA graph of one device build (lai_jk_opts.graph) and what it was captured for
   struct GraphKey {
     const double* D;

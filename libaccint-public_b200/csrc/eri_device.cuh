@@ -125,10 +125,13 @@ __device__ __forceinline__ SysMats sys_mats(const JKArgs& args, const QuartetBlo
 // One ket primitive pair's data, loaded a loop iteration ahead of its use so the
 // global-memory latency overlaps the previous primitive's arithmetic (fields a
 // class never reads are removed by the compiler).
-struct KetPrim {
-  double q, eta, he, px, py, pz, qcx, qcy, qcz, c;
+template <typename T>
+struct KetPrimT {
+  T q, eta, he, px, py, pz, qcx, qcy, qcz, c;
 };
-__device__ __forceinline__ void load_ket_prim(const double* __restrict__ pk, size_t sk, KetPrim& k) {
+using KetPrim = KetPrimT<double>;
+template <typename T>
+__device__ __forceinline__ void load_ket_prim(const T* __restrict__ pk, size_t sk, KetPrimT<T>& k) {
   k.q = __ldg(pk + PF_Q * sk);
   k.eta = __ldg(pk + PF_ZETA * sk);
   k.he = __ldg(pk + PF_HZ * sk);
@@ -140,6 +143,15 @@ __device__ __forceinline__ void load_ket_prim(const double* __restrict__ pk, siz
   k.qcz = __ldg(pk + PF_PAZ * sk);
   k.c = __ldg(pk + PF_C * sk);
 }
+
+// Primitive-pair table of a class in the kernel's compute type: the FP64 table,
+// or its FP32 copy for the FP32 kernels.
+template <typename R>
+__device__ __forceinline__ const R* prim_table(const PairClassDev& c);
+template <>
+__device__ __forceinline__ const double* prim_table<double>(const PairClassDev& c) { return c.prim; }
+template <>
+__device__ __forceinline__ const float* prim_table<float>(const PairClassDev& c) { return c.primf; }
 
 // Bra primitive-pair data of one pair (same fields, bra side).
 struct BraPrim {

@@ -26,6 +26,11 @@ int launch_sliced(const QuartetBlock& blk, const JKArgs& args, const RysTablesVi
                   cudaStream_t stream, bool fp32, int num_sms);
 bool sliced_class_supported(int la, int lb, int lc, int ld);
 
+// Warp-per-quartet kernel with lanes over the output integrals (eri_tiled.cu),
+// any class with l <= 4; 0 on success, -1 if the class does not fit shared memory.
+int launch_tiled(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
+                 int num_sms);
+
 // Warp-per-quartet generic kernel (eri_generic.cu), any class with l <= 4.
 int launch_generic(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
                    cudaStream_t stream, double* gscratch, size_t gscratch_doubles, int num_sms);

@@ -77,35 +77,37 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   const int ib0 = SPLIT ? sub : 0, ibs = SPLIT ? ps : 1;
   // One primitive quartet: bra primitive pair (zeta, hz, P, PA, cab), ket
   // primitive pair `cur`; accumulates into G.
+  // Pair data in the compute type: the FP32 kernels read an FP32 copy of the
+  // tables (half the bytes and registers, no conversions).  Their P - Q is then
+  // formed in FP32: an absolute error ~1e-7 |P| that moves T by ~1e-6 relative at
+  // worst, inside the FP32 error of the quartets the cut sends to this path.
+  const R* __restrict__ bprim = prim_table<R>(blk.bra);
+  const R* __restrict__ kprim = prim_table<R>(blk.ket);
   struct BraVals {
-    R zeta, hz;
-    double Px, Py, Pz;
-    R PAx, PAy, PAz, cab;
+    R zeta, hz, Px, Py, Pz, PAx, PAy, PAz, cab;
   };
-  auto load_bra = [&](int ib, double& qab, BraVals& v) {
-    const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
+  auto load_bra = [&](int ib, R& qab, BraVals& v) {
+    const R* pb = bprim + (size_t)ib * nbra + p;
     qab = __ldg(pb + PF_Q * sb);
-    v.zeta = R(__ldg(pb + PF_ZETA * sb));
-    v.hz = R(__ldg(pb + PF_HZ * sb));
-    // P - Q is formed in FP64 on both paths: the centres are O(10) bohr, and their
-    // FP32 difference would lose the digits that T = rho |PQ|^2 needs
+    v.zeta = __ldg(pb + PF_ZETA * sb);
+    v.hz = __ldg(pb + PF_HZ * sb);
     v.Px = __ldg(pb + PF_PX * sb);
     v.Py = __ldg(pb + PF_PY * sb);
     v.Pz = __ldg(pb + PF_PZ * sb);
-    v.PAx = R(__ldg(pb + PF_PAX * sb));
-    v.PAy = R(__ldg(pb + PF_PAY * sb));
-    v.PAz = R(__ldg(pb + PF_PAZ * sb));
-    v.cab = R(__ldg(pb + PF_C * sb));
+    v.PAx = __ldg(pb + PF_PAX * sb);
+    v.PAy = __ldg(pb + PF_PAY * sb);
+    v.PAz = __ldg(pb + PF_PAZ * sb);
+    v.cab = __ldg(pb + PF_C * sb);
   };
-  auto prim = [&](const BraVals& bv, const KetPrim& cur) {
+  auto prim = [&](const BraVals& bv, const KetPrimT<R>& cur) {
     const R zeta = bv.zeta, hz = bv.hz, cab = bv.cab;
-    const double Px = bv.Px, Py = bv.Py, Pz = bv.Pz;
+    const R Px = bv.Px, Py = bv.Py, Pz = bv.Pz;
     const R PAx = bv.PAx, PAy = bv.PAy, PAz = bv.PAz;
     const R eta = R(cur.eta);
     const R he = R(cur.he);
-    const R PQx = R(Px - cur.px);
-    const R PQy = R(Py - cur.py);
-    const R PQz = R(Pz - cur.pz);
+    const R PQx = Px - cur.px;
+    const R PQy = Py - cur.py;
+    const R PQz = Pz - cur.pz;
     const R QCx = R(cur.qcx), QCy = R(cur.qcy), QCz = R(cur.qcz);
     const R ccd = R(cur.c);
     const R s = zeta + eta;
@@ -187,35 +189,37 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   // primitives (s pairs against p/d pairs) and goes inside, with its next primitive
   // pair loaded one iteration ahead.
   constexpr bool kKetOuter = (LAB == LCD);
-  const double* pk0 = blk.ket.prim + q;
+  const R* pk0 = kprim + q;
+  const R peps_r = R(peps);
   if constexpr (kKetOuter) {
-    const double qab_max = ib0 < Kab ? __ldg(blk.bra.prim + (size_t)ib0 * nbra + p + PF_Q * sb) : 0.0;
-    KetPrim nxt;
+    const R qab_max = ib0 < Kab ? __ldg(bprim + (size_t)ib0 * nbra + p + PF_Q * sb) : R(0);
+    KetPrimT<R> nxt;
     load_ket_prim(pk0, sk, nxt);
     for (int ik = 0; ik < Kcd; ++ik) {
-      const KetPrim cur = nxt;
-      if (qab_max * cur.q < peps || ib0 >= Kab) break;
+      const KetPrimT<R> cur = nxt;
+      if (qab_max * cur.q < peps_r || ib0 >= Kab) break;
       if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
       for (int ib = ib0; ib < Kab; ib += ibs) {
-        double qab;
+        R qab;
         BraVals bv;
         load_bra(ib, qab, bv);
-        if (qab * cur.q < peps) break;
+        if (qab * cur.q < peps_r) break;
         ++nprim_done;
         prim(bv, cur);
       }
     }
   } else {
+    const R qket_max = R(blk.ket.qprim_max);
     for (int ib = ib0; ib < Kab; ib += ibs) {
-      double qab;
+      R qab;
       BraVals bv;
       load_bra(ib, qab, bv);
-      if (qab * blk.ket.qprim_max < peps) break;
-      KetPrim nxt;
+      if (qab * qket_max < peps_r) break;
+      KetPrimT<R> nxt;
       load_ket_prim(pk0, sk, nxt);
       for (int ik = 0; ik < Kcd; ++ik) {
-        const KetPrim cur = nxt;
-        if (qab * cur.q < peps) break;
+        const KetPrimT<R> cur = nxt;
+        if (qab * cur.q < peps_r) break;
         if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
         ++nprim_done;
         prim(bv, cur);
@@ -466,12 +470,19 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
 }
 
 // Blocks per SM the register allocation must allow (ptxas caps registers at
-// 65536 / (256 * blocks)).  The one-root classes are latency bound with short
-// dependent chains and need the warps: (ss|ss) fits 64 registers (4 blocks, 32
-// warps), (ps|ss) 80 (3 blocks).  The other classes keep ptxas's own choice (0 =
-// no bound; an explicit 1 would let it take up to 255 registers).
+// 65536 / (256 * blocks)).  The light classes are latency bound with short
+// dependent chains and need the warps: in FP64 (ss|ss) fits 64 registers (4
+// blocks, 32 warps) and (ps|ss) 80 (3 blocks); in FP32 the one-root classes fit 64
+// and the L = 2 ones 80.  The other classes keep ptxas's own choice (0 = no bound;
+// an explicit 1 would let it take up to 255 registers).
+template <int LA, int LB, int LC, int LD, typename R>
+__host__ __device__ constexpr int small_min_blocks() {
+  constexpr int L = LA + LB + LC + LD;
+  return sizeof(R) == 8 ? (L == 0 ? 4 : L == 1 ? 3 : 0) : (L <= 1 ? 4 : L == 2 ? 3 : 0);
+}
+
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>
-__global__ void __launch_bounds__(256, (LA + LB + LC + LD == 0 ? 4 : LA + LB + LC + LD == 1 ? 3 : 0))
+__global__ void __launch_bounds__(256, (small_min_blocks<LA, LB, LC, LD, R>()))
     eri_small_kernel(QuartetBlock blk, JKArgs args, RysTablesView tab, int kSuper, int ps) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -552,11 +563,10 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
   const int64_t want = (nchunks + (threads / 32) - 1) / (threads / 32);
   const int64_t cap = (int64_t)num_sms * per_sm;
   const int grid = (int)(want < cap ? want : cap);
-  // chunks per super-chunk: long runs (one bra search each) when the launch has
-  // plenty of work, short ones when it would otherwise leave warps idle
-  const int64_t warps_total = (int64_t)grid * (threads / 32);
-  const int ksuper = tune.ksuper > 0 ? tune.ksuper
-                                     : (int)std::max<int64_t>(1, std::min<int64_t>(16, nchunks / (8 * warps_total)));
+  // chunks per super-chunk (consecutive chunks a warp takes, one bra search per
+  // super-chunk): the autotuner chose 1 for most launches of the benchmark
+  // systems (longer runs load-balance worse), so 1 is the default
+  const int ksuper = tune.ksuper > 0 ? tune.ksuper : 1;
   kern<<<grid, threads, smem, stream>>>(blk, args, tab, ksuper, ps);
   return cudaGetLastError() == cudaSuccess ? 1 : -3;
 }

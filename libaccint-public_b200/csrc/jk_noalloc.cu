@@ -13,8 +13,6 @@
 // Limits and rules (also in include/libaccint_b200.h):
 //   * nbf <= LAI_NOALLOC_MAX_NBF (512): the array holds 2 x 512 x 512 doubles
 //     (4 MiB), resident on every GPU that loads the library until the process ends;
-//   * bases with a class whose (e0|f0) block needs global scratch (the largest
-//     g-function classes) are rejected;
 //   * all calls share the array: calls whose device work overlaps (different
 //     streams, or different engines on one device) race; serialize them;
 //   * the first call on a device looks up the array's device address (host code
@@ -81,14 +79,6 @@ extern "C" int lai_jk_build_noalloc(lai_engine* engine, const double* d_D, doubl
   if (cudaSetDevice(dev) != cudaSuccess) return err(LAI_ECUDA, "lai_jk_build_noalloc: cudaSetDevice");
   const int nb = lai::engine_block_count(engine);
   const int sms = lai::engine_num_sms(engine);
-  for (int b = 0; b < nb; ++b) {
-    const lai::QuartetBlock q = lai::engine_block(engine, b);
-    const int la = q.bra.la, lb = q.bra.lb, lc = q.ket.la, ld = q.ket.lb;
-    if (!lai::small_class_supported(la, lb, lc, ld) && !lai::sliced_class_supported(la, lb, lc, ld) &&
-        lai::generic_global_scratch_doubles(la, lb, lc, ld, sms) > 0)
-      return err(LAI_ENOTSUP, "lai_jk_build_noalloc: a shell-quartet class of this basis needs "
-                              "global scratch; use lai_jk_build_device");
-  }
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_addr_mutex);
@@ -121,7 +111,7 @@ extern "C" int lai_jk_build_noalloc(lai_engine* engine, const double* d_D, doubl
     else if (lai::sliced_class_supported(la, lb, lc, ld))
       rc = lai::launch_sliced(q, args, tab, s, false, sms) == 1 ? 0 : -1;
     else
-      rc = lai::launch_generic(q, args, tab, s, nullptr, 0, sms);
+      rc = lai::launch_tiled(q, args, tab, s, sms);
     if (rc < 0) return err(LAI_ECUDA, "lai_jk_build_noalloc: kernel launch failed");
   }
   if (nn > 0)

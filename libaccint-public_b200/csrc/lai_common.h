@@ -54,6 +54,7 @@ struct PairClassDev {
   const double* prim;  // [PF_COUNT * Ka*Kb * npairs]
   double qprim_max;    // largest PF_Q of the class
   const int* sys;      // [npairs] system of each pair in a batched engine, else nullptr
+  const float* primf;  // FP32 copy of prim (the FP32 kernels of mixed precision)
 };
 
 // One launch: the canonical quartets (p, q) with p a pair of class `bra` and q a

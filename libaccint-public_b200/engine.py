@@ -18,6 +18,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
+from .basis import point_charges
 
 
 class Operator:
@@ -260,6 +261,59 @@ class Engine:
         g = np.zeros((self.natom(), 3))
         _lib.check(_lib.lib().lai_jk_gradient(self._h, D.ctypes.data, n, g.ctypes.data))
         return g
+
+    # --- one-electron integrals: Engine::compute_overlap_matrix / compute_kinetic_matrix /
+    # compute_nuclear_matrix (include/libaccint/engine/engine.hpp:831-900; Python
+    # bindings python/src/engine_bindings.cpp:146-200) ---
+    def _charges(self, atoms):
+        if atoms is None:
+            atoms = self.basis.atoms
+            if atoms is None:
+                raise ValueError("nuclear attraction needs atoms (the basis was not built from atoms)")
+        return point_charges(atoms)
+
+    def _one_electron(self, op, atoms=None):
+        n = self.basis.nbf
+        out = np.empty((n, n))
+        xyz = q = None
+        nc = 0
+        if op in (_lib.LAI_OP_NUCLEAR, _lib.LAI_OP_HCORE):
+            xyz, q = self._charges(atoms)
+            nc = len(q)
+        _lib.check(_lib.lib().lai_one_electron(self._h, op, nc, None if xyz is None else xyz.ctypes.data,
+                                                None if q is None else q.ctypes.data, out.ctypes.data))
+        return out
+
+    def compute_overlap_matrix(self):
+        """S (nbf x nbf)."""
+        return self._one_electron(_lib.LAI_OP_OVERLAP)
+
+    def compute_kinetic_matrix(self):
+        """T (nbf x nbf)."""
+        return self._one_electron(_lib.LAI_OP_KINETIC)
+
+    def compute_nuclear_matrix(self, atoms=None):
+        """V (nbf x nbf) of the nuclei (list of Atom / (Z, xyz) pairs, or
+        PointChargeParams-like); default: the atoms the basis was built on."""
+        return self._one_electron(_lib.LAI_OP_NUCLEAR, atoms)
+
+    def compute_core_hamiltonian(self, atoms=None):
+        """H_core = T + V in one call."""
+        return self._one_electron(_lib.LAI_OP_HCORE, atoms)
+
+    def one_electron_device(self, op, d_out, atoms=None, stream=0):
+        """op in {"overlap", "kinetic", "nuclear", "hcore"} into the device buffer
+        d_out (nbf x nbf doubles), asynchronous on stream."""
+        code = {"overlap": _lib.LAI_OP_OVERLAP, "kinetic": _lib.LAI_OP_KINETIC,
+                "nuclear": _lib.LAI_OP_NUCLEAR, "hcore": _lib.LAI_OP_HCORE}[op]
+        xyz = q = None
+        nc = 0
+        if code in (_lib.LAI_OP_NUCLEAR, _lib.LAI_OP_HCORE):
+            xyz, q = self._charges(atoms)
+            nc = len(q)
+        _lib.check(_lib.lib().lai_one_electron_device(
+            self._h, code, nc, None if xyz is None else xyz.ctypes.data,
+            None if q is None else q.ctypes.data, ctypes.c_void_p(d_out), ctypes.c_void_p(stream)))
 
     def compute_and_consume(self, op, consumer, screening=None):
         if not op.is_two_electron():

@@ -47,6 +47,7 @@ def restatement():
         L.orc_schwarz.argtypes = [_I, _P, _P, _P, _P, _P, _P]
         L.orc_jk_sym.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _D]
         L.orc_jk_sym.restype = ctypes.c_long
+        L.orc_one_electron.argtypes = [_I, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P]
         _orc = L
     return _orc
 
@@ -83,6 +84,8 @@ def reference():
         L.ref_max_threads.restype = _I
         L.ref_cart_to_sph.restype = _I
         L.ref_cart_to_sph.argtypes = [_I, _P]
+        L.ref_one_electron.restype = _I
+        L.ref_one_electron.argtypes = [_P, _I, _I, _P, _P, _P]
         _ref = L
     return _ref
 
@@ -178,6 +181,94 @@ def orc_schwarz(basis):
     return Q
 
 
+def orc_one_electron(basis, kind, xyz=None, q=None):
+    """kind 0 S, 1 T, 2 V (point charges xyz [n][3], q [n]) by the McMurchie-Davidson
+    restatement in rys_oracle.c."""
+    O = restatement()
+    l, nprim, centers, exps, coefs = normalized_arrays(basis)
+    n = basis.nbf
+    out = np.zeros((n, n))
+    nc = 0
+    if kind == 2:
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        nc = len(q)
+    rc = O.orc_one_electron(len(l), l.ctypes.data, nprim.ctypes.data, centers.ctypes.data, exps.ctypes.data,
+                            coefs.ctypes.data, kind, nc, None if xyz is None else xyz.ctypes.data,
+                            None if q is None else q.ctypes.data, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("orc_one_electron failed")
+    return out
+
+
+def nuclear_repulsion(Z, xyz):
+    xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
+    e = 0.0
+    for i in range(len(Z)):
+        for j in range(i + 1, len(Z)):
+            e += float(Z[i]) * float(Z[j]) / float(np.linalg.norm(xyz[i] - xyz[j]))
+    return e
+
+
+def orc_rhf(S, H, jk, nocc, enuc, energy_threshold=1e-12, density_threshold=1e-10, max_iterations=100,
+            diis_size=6):
+    """Restricted Hartree-Fock in numpy, step for step the driver of the reference's
+    tests/integration/test_hf_energy.cpp:64-294: symmetric orthogonalization
+    X = U s^-1/2 U^T (eigenvalues <= 1e-10 dropped), core-Hamiltonian guess,
+    D = 2 C_occ C_occ^T, F = H + J - K/2, E = 1/2 tr((H + F) D) + E_nuc, DIIS on
+    e = F D S - S D F (last 6), convergence |dE| < 1e-12 and max |dD| < 1e-10 after
+    the first iteration, final energy from a fresh build at the converged D.
+    jk(D) -> (J, K).  Returns (E, iterations, converged)."""
+    s, U = np.linalg.eigh(S)
+    sinv = np.where(s > 1e-10, 1.0 / np.sqrt(np.where(s > 1e-10, s, 1.0)), 0.0)
+    X = (U * sinv) @ U.T
+
+    def solve(F):
+        e, Cp = np.linalg.eigh(X.T @ F @ X)
+        return X @ Cp
+
+    def density(C):
+        Co = C[:, :nocc]
+        return 2.0 * Co @ Co.T
+
+    D = density(solve(H))
+    E_old = 0.0
+    fs, es = [], []
+    for it in range(max_iterations):
+        J, K = jk(D)
+        F = H + J - 0.5 * K
+        E = 0.5 * float(np.sum((H + F) * D)) + enuc
+        err = F @ D @ S - S @ D @ F
+        fs.append(F)
+        es.append(err)
+        if len(fs) > diis_size:
+            fs.pop(0)
+            es.pop(0)
+        if len(fs) < 2:
+            Fd = fs[-1]
+        else:
+            m = len(fs)
+            B = np.zeros((m + 1, m + 1))
+            for i in range(m):
+                for j in range(m):
+                    B[i, j] = float(np.sum(es[i] * es[j]))
+            B[m, :m] = B[:m, m] = -1.0
+            rhs = np.zeros(m + 1)
+            rhs[m] = -1.0
+            c = np.linalg.lstsq(B, rhs, rcond=None)[0]
+            Fd = sum(c[i] * fs[i] for i in range(m))
+        Dn = density(solve(Fd))
+        dD = float(np.max(np.abs(Dn - D)))
+        if abs(E - E_old) < energy_threshold and dD < density_threshold and it > 0:
+            D = Dn
+            J, K = jk(D)
+            F = H + J - 0.5 * K
+            return 0.5 * float(np.sum((H + F) * D)) + enuc, it + 1, True
+        D = Dn
+        E_old = E
+    return E_old, max_iterations, False
+
+
 def orc_rys(n, T):
     O = restatement()
     u = np.zeros(n)
@@ -266,6 +357,22 @@ class RefBasis:
         if t < 0:
             raise RuntimeError(self.R.ref_last_error().decode())
         return t, J, K
+
+    def one_electron(self, kind, xyz=None, q=None):
+        """kind 0 S, 1 T, 2 V of the point charges: the reference CPU engine's
+        compute_overlap_matrix / compute_kinetic_matrix / compute_nuclear_matrix."""
+        n = self.nbf
+        out = np.zeros((n, n))
+        nc = 0
+        if kind == 2:
+            xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+            q = np.ascontiguousarray(q, dtype=np.float64)
+            nc = len(q)
+        rc = self.R.ref_one_electron(self.h, kind, nc, None if xyz is None else xyz.ctypes.data,
+                                     None if q is None else q.ctypes.data, out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(self.R.ref_last_error().decode())
+        return out
 
     def shell_info(self, i):
         l = ctypes.c_int()

@@ -18,6 +18,8 @@
 //                                             src/shared/math/boys_function.cpp:253-303
 //   - FockBuilder::accumulate_symmetric       src/shared/consumers/fock_builder.cpp:123-222
 //   - math::get_cart_to_sph_matrix            include/libaccint/math/spherical_transform.hpp:20-40
+//   - Engine::compute_overlap_matrix / compute_kinetic_matrix / compute_nuclear_matrix
+//                                             include/libaccint/engine/engine.hpp:831-900
 #include <libaccint/libaccint.hpp>
 #include <libaccint/engine/engine.hpp>
 #include <libaccint/consumers/fock_builder.hpp>
@@ -310,6 +312,37 @@ int ref_cart_to_sph(int l, double* out) {
         const int n = (2 * l + 1) * (l + 1) * (l + 2) / 2;
         std::memcpy(out, C, sizeof(double) * n);
         return n;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1;
+    }
+}
+
+// One-electron matrix of the reference CPU engine: kind 0 overlap, 1 kinetic,
+// 2 nuclear attraction of the point charges (xyz [n][3], q [n]).  Returns 0 or -1.
+int ref_one_electron(void* h, int kind, int ncharge, const double* xyz, const double* q, double* out) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(h)->basis;
+        const Size n = basis.n_basis_functions();
+        Engine engine(basis);
+        std::vector<Real> r;
+        if (kind == 0) {
+            engine.compute_overlap_matrix(r, BackendHint::ForceCPU);
+        } else if (kind == 1) {
+            engine.compute_kinetic_matrix(r, BackendHint::ForceCPU);
+        } else {
+            PointChargeParams c;
+            for (int i = 0; i < ncharge; ++i) {
+                c.x.push_back(xyz[3 * i]);
+                c.y.push_back(xyz[3 * i + 1]);
+                c.z.push_back(xyz[3 * i + 2]);
+                c.charge.push_back(q[i]);
+            }
+            engine.compute_nuclear_matrix(c, r, BackendHint::ForceCPU);
+        }
+        if (r.size() != n * n) { set_err("ref_one_electron: unexpected result size"); return -1; }
+        std::memcpy(out, r.data(), sizeof(double) * n * n);
+        return 0;
     } catch (const std::exception& ex) {
         set_err(ex.what());
         return -1;

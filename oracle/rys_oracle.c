@@ -501,3 +501,148 @@ long orc_jk_sym(int n, const int *l, const int *nprim, const double *ctr, const 
     basis_free(&b);
     return count;
 }
+
+/* ------------------------------------------------------------------------- */
+/* One-electron integrals by McMurchie-Davidson Hermite expansion: a method   */
+/* independent of the Obara-Saika/Rys recurrences of both the reference       */
+/* (src/host/kernels/{overlap,kinetic,nuclear}_kernel.cpp) and the CUDA path, */
+/* with the Boys function F_n(T) in binary128 (boys_q).                       */
+/*   E^{i+1,j}_t = E^{ij}_{t-1}/(2p) + PA E^{ij}_t + (t+1) E^{ij}_{t+1}        */
+/*   E^{i,j+1}_t = E^{ij}_{t-1}/(2p) + PB E^{ij}_t + (t+1) E^{ij}_{t+1}        */
+/*   s_ij = E^{ij}_0 sqrt(pi/p) exp(-mu X_AB^2)                               */
+/*   t_ij = 1/2 [ i j s_{i-1,j-1} - 2 a j s_{i+1,j-1} - 2 b i s_{i-1,j+1}     */
+/*               + 4 a b s_{i+1,j+1} ]   (symmetric derivative form)          */
+/*   V_ab = -q (2 pi/p) K_AB sum_tuv E_t E_u E_v R_tuv,                       */
+/*   R^n_000 = (-2p)^n F_n(p PC^2), R^n_{t+1,u,v} = t R^{n+1}_{t-1,u,v}       */
+/*             + PC_x R^{n+1}_{t,u,v} (same for u, v).                        */
+/* ------------------------------------------------------------------------- */
+#define MD_L (2 * ORC_MAX_L + 3)
+static void md_e(int imax, int jmax, double pa, double pb, double p, double E[MD_L][MD_L][2 * MD_L]) {
+    memset(E, 0, sizeof(double) * MD_L * MD_L * 2 * MD_L);
+    E[0][0][0] = 1.0;
+    const double h = 0.5 / p;
+    for (int i = 0; i <= imax; ++i)
+        for (int j = 0; j <= jmax; ++j) {
+            if (i == 0 && j == 0) continue;
+            for (int t = 0; t <= i + j; ++t) {
+                double v;
+                if (i > 0) {
+                    const double (*e)[2 * MD_L] = E[i - 1];
+                    v = pa * e[j][t] + (t + 1) * e[j][t + 1] + (t > 0 ? h * e[j][t - 1] : 0.0);
+                } else {
+                    const double *e = E[i][j - 1];
+                    v = pb * e[t] + (t + 1) * e[t + 1] + (t > 0 ? h * e[t - 1] : 0.0);
+                }
+                E[i][j][t] = v;
+            }
+        }
+}
+
+/* Hermite Coulomb integrals R_{tuv} (n = 0) for t+u+v <= L. */
+static void md_r(int L, double p, double x, double y, double z, double *R /* [L+1]^3 */) {
+    const int d = L + 1;
+    double *W = calloc((size_t)(L + 1) * d * d * d, sizeof(double));
+#define RW(n, t, u, v) W[(((n) * d + (t)) * d + (u)) * d + (v)]
+    q_t F[ORC_MAX_MOM + 8];
+    boys_q(L, (q_t)(p * (x * x + y * y + z * z)), F);
+    double m = 1.0;
+    for (int n = 0; n <= L; ++n) { RW(n, 0, 0, 0) = m * (double)F[n]; m *= -2.0 * p; }
+    for (int n = L - 1; n >= 0; --n)
+        for (int s = 1; s <= L - n; ++s)
+            for (int t = 0; t <= s; ++t)
+                for (int u = 0; u <= s - t; ++u) {
+                    const int v = s - t - u;
+                    double r;
+                    if (t > 0) r = x * RW(n + 1, t - 1, u, v) + (t > 1 ? (t - 1) * RW(n + 1, t - 2, u, v) : 0.0);
+                    else if (u > 0) r = y * RW(n + 1, t, u - 1, v) + (u > 1 ? (u - 1) * RW(n + 1, t, u - 2, v) : 0.0);
+                    else r = z * RW(n + 1, t, u, v - 1) + (v > 1 ? (v - 1) * RW(n + 1, t, u, v - 2) : 0.0);
+                    RW(n, t, u, v) = r;
+                }
+    for (int t = 0; t <= L; ++t)
+        for (int u = 0; u <= L; ++u)
+            for (int v = 0; v <= L; ++v) R[(t * d + u) * d + v] = (t + u + v <= L) ? RW(0, t, u, v) : 0.0;
+#undef RW
+    free(W);
+}
+
+/* kind 0 overlap, 1 kinetic, 2 nuclear (charges xyz [nc][3], q [nc]); out nbf x nbf. */
+int orc_one_electron(int n, const int *l, const int *nprim, const double *ctr, const double *exps,
+                     const double *coefs, int kind, int nc, const double *xyz, const double *q,
+                     double *out) {
+    basis_t b;
+    basis_init(&b, n, l, nprim, ctr, exps, coefs);
+    const long nbf = b.foff[n];
+    static double E[3][MD_L][MD_L][2 * MD_L];
+    for (int s1 = 0; s1 < n; ++s1)
+        for (int s2 = 0; s2 < n; ++s2) {
+            const int la = l[s1], lb = l[s2], na = ncart(la), nb = ncart(lb);
+            if (la > ORC_MAX_L || lb > ORC_MAX_L) { basis_free(&b); return -1; }
+            int ca[28][3], cb[28][3];
+            cart_list(la, ca);
+            cart_list(lb, cb);
+            const double *A = ctr + 3 * s1, *B = ctr + 3 * s2;
+            double *blk = calloc((size_t)na * nb, sizeof(double));
+            for (int i1 = 0; i1 < nprim[s1]; ++i1)
+                for (int i2 = 0; i2 < nprim[s2]; ++i2) {
+                    const double al = exps[b.poff[s1] + i1], be = exps[b.poff[s2] + i2];
+                    const double c = coefs[b.poff[s1] + i1] * coefs[b.poff[s2] + i2];
+                    const double p = al + be, mu = al * be / p;
+                    double P[3], K = 1.0;
+                    for (int x = 0; x < 3; ++x) {
+                        P[x] = (al * A[x] + be * B[x]) / p;
+                        K *= exp(-mu * (A[x] - B[x]) * (A[x] - B[x]));
+                        md_e(la + 1, lb + 1, P[x] - A[x], P[x] - B[x], p, E[x]);
+                    }
+                    const double sp = sqrt(M_PI / p);
+                    if (kind == 0 || kind == 1) {
+                        for (int ia = 0; ia < na; ++ia)
+                            for (int ib = 0; ib < nb; ++ib) {
+                                double s[3], t[3];
+                                for (int x = 0; x < 3; ++x) {
+                                    const int i = ca[ia][x], j = cb[ib][x];
+                                    s[x] = E[x][i][j][0] * sp;
+                                    if (kind == 1) {
+                                        double v = 4 * al * be * E[x][i + 1][j + 1][0];
+                                        if (j > 0) v -= 2 * al * j * E[x][i + 1][j - 1][0];
+                                        if (i > 0) v -= 2 * be * i * E[x][i - 1][j + 1][0];
+                                        if (i > 0 && j > 0) v += i * j * E[x][i - 1][j - 1][0];
+                                        t[x] = 0.5 * v * sp;
+                                    }
+                                }
+                                double v = kind == 0 ? s[0] * s[1] * s[2]
+                                                     : t[0] * s[1] * s[2] + s[0] * t[1] * s[2] + s[0] * s[1] * t[2];
+                                blk[ia * nb + ib] += c * K * v;
+                            }
+                    } else {
+                        const int L = la + lb, d = L + 1;
+                        double *R = malloc(sizeof(double) * d * d * d);
+                        for (int ic = 0; ic < nc; ++ic) {
+                            md_r(L, p, P[0] - xyz[3 * ic], P[1] - xyz[3 * ic + 1], P[2] - xyz[3 * ic + 2], R);
+                            const double f = -q[ic] * 2 * M_PI / p * c * K;
+                            for (int ia = 0; ia < na; ++ia)
+                                for (int ib = 0; ib < nb; ++ib) {
+                                    const int ix = ca[ia][0], jx = cb[ib][0], iy = ca[ia][1], jy = cb[ib][1],
+                                              iz = ca[ia][2], jz = cb[ib][2];
+                                    double v = 0.0;
+                                    for (int t = 0; t <= ix + jx; ++t)
+                                        for (int u = 0; u <= iy + jy; ++u)
+                                            for (int w = 0; w <= iz + jz; ++w)
+                                                v += E[0][ix][jx][t] * E[1][iy][jy][u] * E[2][iz][jz][w] *
+                                                     R[(t * d + u) * d + w];
+                                    blk[ia * nb + ib] += f * v;
+                                }
+                        }
+                        free(R);
+                    }
+                }
+            for (int ia = 0; ia < na; ++ia)
+                for (int ib = 0; ib < nb; ++ib) {
+                    const double nrm = 1.0 / sqrt(dfact_odd(ca[ia][0]) * dfact_odd(ca[ia][1]) * dfact_odd(ca[ia][2]) *
+                                                  dfact_odd(cb[ib][0]) * dfact_odd(cb[ib][1]) * dfact_odd(cb[ib][2]));
+                    out[(b.foff[s1] + ia) * nbf + b.foff[s2] + ib] = blk[ia * nb + ib] * nrm;
+                }
+            free(blk);
+        }
+    basis_free(&b);
+    return 0;
+}

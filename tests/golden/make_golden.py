@@ -15,6 +15,12 @@ Fixtures and their provenance:
                          FockBuilder) (full N^4, no screening), for the seeded
                          workloads h2o8_sto3g (config 0: built-in STO-3G, 8 waters)
                          and h2o2_ccpvdz, plus the density used.
+* one_electron_sto3g.npz -- tests/integration/test_one_electron.cpp of the reference
+                         (PySCF cart=True values written into the test): the H2 and
+                         H2O STO-3G shells, point charges and S, T, V matrices; and
+                         tests/integration/test_hf_energy.cpp: RHF total energies of
+                         H2, H2O and CH4 with the built-in STO-3G (PySCF) and the H2O
+                         nuclear repulsion.  Parsed from the test sources as text.
 * eri_ccpvqz_samples.npz -- per-integral values of sampled shell quartets of all
                          angular-momentum classes present in an H2O + CH4 pair with
                          cc-pVQZ (up to g): the reference's compute_eri and the
@@ -133,8 +139,76 @@ def eri_samples(nsample=400, seed=3):
                         flat=np.array(flat), ref=np.concatenate(ref_vals), orc=np.concatenate(orc_vals))
 
 
+def _floats(txt):
+    import re
+    return [float(x) for x in re.findall(r"[-+]?\d+\.\d*(?:[eE][-+]?\d+)?", txt)]
+
+
+def one_electron():
+    import re
+    src = open(os.path.join(REF, "tests/integration/test_one_electron.cpp")).read()
+    out = {}
+    for arr in ("H2_S_REF", "H2_T_REF", "H2_V_REF", "H2O_S_REF", "H2O_T_REF", "H2O_V_REF"):
+        m = re.search(r"constexpr Real %s\[(\d+)\] = \{(.*?)\};" % arr, src, re.S)
+        body = "\n".join(line.split("//")[0] for line in m.group(2).splitlines())
+        vals = _floats(body)
+        assert len(vals) == int(m.group(1)), arr
+        n = int(round(len(vals) ** 0.5))
+        out[arr] = np.array(vals).reshape(n, n)
+    # shells of make_h2_sto3g / make_h2o_sto3g
+    vecs = {k: _floats(v) for k, v in re.findall(r"std::vector<Real> (\w+) = \{([^}]*)\};", src)}
+    for name, fn in (("h2", "make_h2_sto3g"), ("h2o", "make_h2o_sto3g")):
+        body = src[src.index("BasisSet %s()" % fn):]
+        body = body[:body.index("return BasisSet")]
+        pts = {k: _floats(v) for k, v in re.findall(r"Point3D (\w+)\{([^}]*)\};", body)}
+        ls, ctr, ex, co, npr = [], [], [], [], []
+        for m in re.finditer(r"Shell (\w+)\((\d),\s*(\w+),\s*(\{[^}]*\}|\w+),\s*(\{[^}]*\}|\w+)\);", body):
+            e = _floats(m.group(4)) if m.group(4).startswith("{") else vecs[m.group(4)]
+            c = _floats(m.group(5)) if m.group(5).startswith("{") else vecs[m.group(5)]
+            ls.append(int(m.group(2)))
+            ctr.append(pts[m.group(3)])
+            ex += e
+            co += c
+            npr.append(len(e))
+        out[name + "_l"] = np.array(ls, dtype=np.int32)
+        out[name + "_center"] = np.array(ctr)
+        out[name + "_nprim"] = np.array(npr, dtype=np.int32)
+        out[name + "_exps"] = np.array(ex)
+        out[name + "_coefs"] = np.array(co)
+        cb = src[src.index("PointChargeParams %s_charges()" % fn.replace("_sto3g", "").replace("make_", "make_")):]
+        cb = cb[:cb.index("return charges")]
+        xyz = [_floats(re.search(r"charges\.%s = \{([^}]*)\}" % k, cb).group(1)) for k in "xyz"]
+        out[name + "_charge_xyz"] = np.array(xyz).T.copy()
+        out[name + "_charge_q"] = np.array(_floats(re.search(r"charges\.charge = \{([^}]*)\}", cb).group(1)))
+    hf = open(os.path.join(REF, "tests/integration/test_hf_energy.cpp")).read()
+    for test, key in (("H2O_STO3G", "hf_h2o"), ("H2_STO3G", "hf_h2"), ("CH4_STO3G", "hf_ch4")):
+        body = hf[hf.index("TEST(HFEnergyTest, %s)" % test):]
+        body = body[:body.index("EXPECT_NEAR")]
+        consts = dict((k, float(v)) for k, v in re.findall(r"constexpr Real (\w+) = ([-+0-9.eE]+);", body))
+        atoms = re.findall(r"\{(\d+),\s*\{([^}]*)\}\}", body)
+        Z, xyz = [], []
+        for z, r in atoms:
+            comps = []
+            for tok in r.split(","):
+                tok = tok.strip()
+                sgn = -1.0 if tok.startswith("-") else 1.0
+                tok = tok.lstrip("+-")
+                comps.append(sgn * (consts[tok] if tok in consts else float(tok)))
+            Z.append(int(z))
+            xyz.append(comps)
+        out[key + "_Z"] = np.array(Z, dtype=np.int32)
+        out[key + "_xyz"] = np.array(xyz)
+        out[key + "_energy"] = np.array(consts["REF_ENERGY"])
+        out[key + "_nelec"] = np.array(sum(Z))
+    m = re.search(r"EXPECT_NEAR\(E_nuc, ([-+0-9.eE]+)", hf)
+    out["h2o_enuc"] = np.array(float(m.group(1)))
+    np.savez_compressed(os.path.join(HERE, "one_electron_sto3g.npz"), **out)
+
+
 if __name__ == "__main__":
-    only = sys.argv[2:] if len(sys.argv) > 2 else ["boys", "rys", "water1", "ref", "eri"]
+    only = sys.argv[2:] if len(sys.argv) > 2 else ["boys", "rys", "water1", "ref", "eri", "one"]
+    if "one" in only:
+        one_electron()
     if "boys" in only:
         boys()
     if "rys" in only:
