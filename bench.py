@@ -10,6 +10,10 @@ matching J+K build time.  N > 1 (one process per GPU under torchrun): every rank
 computes an equal slice of every quartet block and one NCCL all-reduce sums J
 and K (strong scaling, total work fixed).
 
+``--workload rhf_<system>`` (e.g. rhf_h2o16_ccpvdz) times a whole device-resident
+RHF calculation instead (one-electron integrals, the J/K build of every iteration,
+DIIS and diagonalization); its metric is seconds per converged SCF.
+
 ``--impl reference`` times the reference's own CPU implementation (the
 unmodified LibAccInt sources compiled into oracle/_ref: compute_2e_shell_quartet
 + FockBuilder::accumulate_symmetric, OpenMP over all host cores) on a seeded
@@ -153,6 +157,10 @@ def time_reference(R, cq, D, target_s, seed):
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
+        return 0
+    if args.workload.startswith("rhf_") or args.workload == "clusters256":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the J/K build of a "
+                          "single system; use --workload h2o64_ccpvdz (default)"}))
         return 0
     lai = importlib.import_module("libaccint-public_b200")
     w = lai.workloads.make(args.workload)
@@ -315,12 +323,54 @@ def run_batched(args):
 # ----------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------
+def run_rhf(args):
+    """Whole RHF calculations (1 GPU; rank 0 only under torchrun): the device
+    driver of libaccint-public_b200/scf.py from the core-Hamiltonian guess to
+    convergence (|dE| < 1e-12, max |dD| < 1e-10)."""
+    import torch
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    lai = importlib.import_module("libaccint-public_b200")
+    name = args.workload[len("rhf_"):]
+    w = lai.workloads.make(name)
+    rhf = lai.scf.RHF(w.basis, threshold=w.thr, device=local)
+    for _ in range(args.warmup):
+        rhf.run()
+    clk = ClockSampler(local)
+    runs = [rhf.run() for _ in range(args.steps)]
+    clk = clk.stop()
+    dev_s = [(r.one_e_ms + sum(r.iter_ms) + r.jk_ms[-1]) * 1e-3 for r in runs]
+    jk_s = [sum(r.jk_ms) * 1e-3 for r in runs]
+    r0 = runs[-1]
+    out = {
+        "metric": "rhf_seconds", "value": statistics.mean(dev_s), "unit": "s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(dev_s),
+        "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "system": SYSTEMS.get(name, name), "nbf": w.nbf,
+                   "electrons": rhf.n_electrons, "schwarz": w.thr,
+                   "convergence": "|dE| < 1e-12 and max |dD| < 1e-10", "diis": 6,
+                   "l2": "inputs larger than L2 for the J/K build (pair data, D/J/K scattered)"},
+        "energy": r0.total_energy, "iterations": r0.iterations, "converged": r0.converged,
+        "jk_share": statistics.mean(j / d for j, d in zip(jk_s, dev_s)),
+        "jk_ms_per_build": statistics.mean(jk_s) * 1e3 / (r0.iterations + 1),
+        "one_electron_ms": r0.one_e_ms,
+        "clocks": clk,
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "clusters256":
         return run_batched(args)
+    if args.workload.startswith("rhf_"):
+        return run_rhf(args)
     import torch
     import torch.distributed as dist
 
