@@ -70,6 +70,15 @@ LAI_API int lai_abi_version(void);
 LAI_API int lai_basis_create(int nshell, const int* l, const int* nprim, const double* centers,
                      const double* exps, const double* coefs, const int* atom_index, int flags,
                      lai_basis** out);
+/* A basis from Basis Set Exchange JSON text (the format of the reference's
+ * share/basis_sets/<name>.json, "complete" or "minimal" schema) on natom atoms with
+ * atomic numbers Z and positions xyz [natom][3] (Bohr); shells per atom in the
+ * file's order, general contractions split into one shell per coefficient column,
+ * SP shells into one shell per l, all-zero columns skipped, raw coefficients
+ * normalized as by lai_basis_create.  Replaces data::BseJsonParser::parse
+ * (src/shared/data/bse_json_parser.cpp:27-140). */
+LAI_API int lai_basis_from_bse_json(const char* json_text, size_t length, int natom, const int* Z,
+                                    const double* xyz, lai_basis** out);
 LAI_API void lai_basis_destroy(lai_basis* basis);
 LAI_API long lai_basis_nbf(const lai_basis* basis);
 LAI_API int lai_basis_nshell(const lai_basis* basis);
@@ -325,14 +334,18 @@ LAI_API int lai_engine_sample_quartets(lai_engine* engine, int64_t n, uint64_t s
 LAI_API int64_t lai_engine_quartet_count(lai_engine* engine);
 /* Autotuner: times every thread-per-quartet class launch of the engine under a
  * few launch configurations (lanes per quartet 1..8, chunks per super-chunk 1, 4,
- * 16) on the device density d_D, and keeps the fastest for later builds.
+ * 16), and every other class launch under each kernel family that covers it
+ * (warp-per-quartet, bra-sliced, tiled), on the device density d_D, and keeps the
+ * fastest for later builds.
  * ms_before/ms_after (may be NULL): summed launch times with the built-in
  * heuristic and with the chosen configurations.  Synchronizes `stream`. */
 LAI_API int lai_engine_autotune(lai_engine* engine, const double* d_D, void* stream, double* ms_before,
                                 double* ms_after);
 /* The launch table: per class-pair block, 10 ints: la, lb, lc, ld, bra and ket
  * primitive pairs per shell pair, quartets (capped at INT32_MAX), tuned lanes per
- * quartet and chunks per super-chunk (0 = heuristic), quartets / 1000.  Returns
+ * quartet (or -1 warp-per-quartet, -2 tiled, -3 bra-sliced kernel for the classes
+ * outside the thread-per-quartet set) and chunks per super-chunk (0 = heuristic),
+ * quartets / 1000.  Returns
  * the block count; rows may be NULL to query it. */
 LAI_API int lai_engine_tune_table(lai_engine* engine, int capacity, int* rows);
 /* FP64 FMA throughput of the device measured by a register-resident FMA loop

@@ -28,7 +28,7 @@ EXPORTED = [
     "lai_engine_natom", "lai_jk_gradient", "lai_jk_gradient_device",
     "lai_engine_create_batched", "lai_engine_batch_layout", "lai_jk_build_batched",
     "lai_engine_autotune", "lai_shard_range", "lai_engine_tune_table",
-    "lai_one_electron", "lai_one_electron_device",
+    "lai_one_electron", "lai_one_electron_device", "lai_basis_from_bse_json",
 ]
 
 LAI_OP_OVERLAP, LAI_OP_KINETIC, LAI_OP_NUCLEAR, LAI_OP_HCORE = 0, 1, 2, 3
@@ -119,6 +119,7 @@ def lib():
         "lai_engine_tune_table": (I, [P, I, P]),
         "lai_one_electron": (I, [P, I, I, P, P, P]),
         "lai_one_electron_device": (I, [P, I, I, P, P, P, P]),
+        "lai_basis_from_bse_json": (I, [ctypes.c_char_p, ctypes.c_size_t, I, P, P, ctypes.POINTER(P)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -28,6 +28,8 @@ def basis_data(name):
     key = name.lower()
     if key in ("sto-3g", "sto3g"):
         key = "sto-3g-builtin"  # the reference's create_builtin_basis("sto-3g") data
+    elif key == "sto-3g-bse":
+        key = "sto-3g"          # the Basis Set Exchange file of the same name
     if key not in _cache:
         raise KeyError(f"basis set {name!r} not bundled (have {sorted(_cache)})")
     return _cache[key]
@@ -109,6 +111,40 @@ class BasisSet:
                 shells.append(Shell(l, r, e, c, a))
         b = cls(shells)
         b.atoms = [Atom(z, r) for z, r in zip(Z, xyz)]
+        return b
+
+    @classmethod
+    def from_bse_json(cls, text, Z, xyz):
+        """A basis from Basis Set Exchange JSON text parsed by the native loader
+        (lai_basis_from_bse_json; data::BseJsonParser::parse of the reference).  The
+        shells are read back from the library, so the Python side mirrors exactly
+        what the C ABI built (coefficients already normalized)."""
+        L = _lib.lib()
+        raw = text.encode() if isinstance(text, str) else bytes(text)
+        Zi = np.ascontiguousarray(Z, dtype=np.int32)
+        R = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        h = ctypes.c_void_p()
+        _lib.check(L.lai_basis_from_bse_json(raw, len(raw), len(Zi), Zi.ctypes.data, R.ctypes.data,
+                                             ctypes.byref(h)))
+        try:
+            shells = []
+            ns = L.lai_basis_nshell(h)
+            for s in range(ns):
+                l_, k_ = ctypes.c_int(), ctypes.c_int()
+                c = np.zeros(3)
+                fi = ctypes.c_long()
+                L.lai_basis_shell(h, s, ctypes.byref(l_), ctypes.byref(k_), c.ctypes.data, None, None,
+                                  ctypes.byref(fi))
+                e = np.zeros(k_.value)
+                cf = np.zeros(k_.value)
+                L.lai_basis_shell(h, s, ctypes.byref(l_), ctypes.byref(k_), c.ctypes.data, e.ctypes.data,
+                                  cf.ctypes.data, ctypes.byref(fi))
+                atom = int(np.argmin(np.linalg.norm(R - c, axis=1))) if len(R) else -1
+                shells.append(Shell(l_.value, c, e, cf, atom))
+        finally:
+            L.lai_basis_destroy(h)
+        b = cls(shells, prenormalized=True)
+        b.atoms = [Atom(z, r) for z, r in zip(Zi, R)]
         return b
 
     # --- flat arrays (the C-ABI layout) ---

@@ -310,7 +310,18 @@ int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs&
                                            cudaGetErrorString(cudaGetLastError()));
     return LAI_OK;
   }
-  if (lai::sliced_class_supported(la, lb, lc, ld)) {
+  // the other classes: warp-per-quartet, bra-sliced or tiled kernel, as tuned for
+  // this block (lai_engine_autotune) or by the measured per-class default; FP32
+  // requests go to the sliced kernel where it exists (the others are FP64 only)
+  int kern = tune.kernel != lai::KERNEL_DEFAULT ? tune.kernel : lai::default_kernel(la, lb, lc, ld);
+  if (fp32 && lai::sliced_class_supported(la, lb, lc, ld)) kern = lai::KERNEL_SLICED;
+  if (kern == lai::KERNEL_WARPQ) {
+    const int rc = lai::launch_warpq(blk, args, E->tab, E->stream, E->num_sms);
+    if (rc == 0) return LAI_OK;
+    if (rc < -1) return fail(LAI_ECUDA, std::string("warp-per-quartet launch failed: ") +
+                                            cudaGetErrorString(lai::warpq_launch_error()));
+  }
+  if (kern != lai::KERNEL_TILED && lai::sliced_class_supported(la, lb, lc, ld)) {
     const int rc = lai::launch_sliced(blk, args, E->tab, E->stream, fp32, E->num_sms);
     if (ran_fp32) *ran_fp32 = fp32;
     if (rc < 0) return fail(LAI_ECUDA, std::string("sliced launch failed: ") +
@@ -1215,7 +1226,23 @@ int lai_engine_autotune(lai_engine* engine, const double* d_D, void* stream, dou
     if ((rc = time_launch(q, bp->tune, &base))) break;
     before += base;
     if (!lai::small_class_supported(q.bra.la, q.bra.lb, q.ket.la, q.ket.lb)) {
-      after += base;
+      // kernel family: warp-per-quartet, bra-sliced, tiled
+      lai::LaunchTune best = bp->tune;
+      float best_ms = base;
+      for (int k : {lai::KERNEL_WARPQ, lai::KERNEL_SLICED, lai::KERNEL_TILED}) {
+        if (k == lai::KERNEL_WARPQ && !lai::warpq_class_supported(q.bra.la, q.bra.lb, q.ket.la, q.ket.lb))
+          continue;
+        if (k == lai::KERNEL_SLICED && !lai::sliced_class_supported(q.bra.la, q.bra.lb, q.ket.la, q.ket.lb))
+          continue;
+        lai::LaunchTune t;
+        t.kernel = k;
+        float m = 0;
+        if ((rc = time_launch(q, t, &m))) break;
+        if (m < 0.98f * best_ms) { best_ms = m; best = t; }
+      }
+      if (rc) break;
+      bp->tune = best;
+      after += best_ms;
       continue;
     }
     const int Kab = q.bra.Ka * q.bra.Kb;
@@ -1252,7 +1279,7 @@ int lai_engine_tune_table(lai_engine* engine, int capacity, int* rows) {
     r[0] = ca.la; r[1] = ca.lb; r[2] = cb.la; r[3] = cb.lb;
     r[4] = ca.Ka * ca.Kb; r[5] = cb.Ka * cb.Kb;
     r[6] = (int)std::min<int64_t>(bp.total, INT32_MAX);
-    r[7] = bp.tune.ps; r[8] = bp.tune.ksuper;
+    r[7] = bp.tune.kernel ? -bp.tune.kernel : bp.tune.ps; r[8] = bp.tune.ksuper;
     r[9] = (int)std::min<int64_t>(bp.total / 1000, INT32_MAX);
   }
   return n;

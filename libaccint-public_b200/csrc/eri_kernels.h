@@ -16,7 +16,10 @@ namespace lai {
 struct LaunchTune {
   int ps = 0;
   int ksuper = 0;
+  int kernel = 0;  // classes outside the thread-per-quartet set: 0 = default choice,
+                   // KERNEL_WARPQ, KERNEL_TILED or KERNEL_SLICED
 };
+enum { KERNEL_DEFAULT = 0, KERNEL_WARPQ = 1, KERNEL_TILED = 2, KERNEL_SLICED = 3 };
 int launch_small(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
                  cudaStream_t stream, bool fp32, int num_sms, LaunchTune tune = LaunchTune{});
 bool small_class_supported(int la, int lb, int lc, int ld);
@@ -28,6 +31,16 @@ bool sliced_class_supported(int la, int lb, int lc, int ld);
 
 // Warp-per-quartet kernel with lanes over the output integrals (eri_tiled.cu),
 // any class with l <= 4; 0 on success, -1 if the class does not fit shared memory.
+// Warp-per-quartet kernel compile-time specialised per class (J/K mode only).
+// Returns 0 when launched, -1 when the class is not instantiated (or the mode is
+// not J/K), < -1 on a CUDA error.
+int launch_warpq(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
+                 int num_sms);
+cudaError_t warpq_launch_error();  // CUDA error of the last failed launch_warpq
+bool warpq_class_supported(int la, int lb, int lc, int ld);
+// Kernel family of a class outside the thread-per-quartet set when no tuned choice
+// exists (measured per class on B200: eri_warpq.cu).
+int default_kernel(int la, int lb, int lc, int ld);
 int launch_tiled(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
                  int num_sms);
 

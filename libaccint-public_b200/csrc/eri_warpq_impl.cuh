@@ -1,0 +1,422 @@
+// Warp-per-quartet Rys ERI kernel, compile-time specialised per class, for the
+// mid-size classes: (dd|pp), (dd|dp), (dd|dd), the d/f classes of triple-zeta
+// bases -- every class whose contracted (e0|f0) block has at most kWarpqMaxG
+// integrals.  J/K digestion only (the raw-integral and Schwarz modes stay on the
+// tiled kernel).
+//
+// Per quartet (one warp), for every primitive quartet:
+//   1. lanes t < 3n (n Rys roots) own (root r = t/3, direction x = t%3): the root,
+//      then the 2D table I_x(e, f), e <= la+lb, f <= lc+ld, by the vertical
+//      recurrence of eri_device.cuh in registers (compile-time indices), stored to
+//      shared memory; the z table carries w_r * prefactor;
+//   2. every lane owns the (e0|f0) integrals j = lane + 32 m of the contracted block
+//      G[e][f] (e over the Cartesian components of shells la..la+lb, f of lc..lc+ld)
+//      and adds sum_r Ix Iy Iz to them in registers.
+// After the last primitive quartet, once per contracted quartet: G goes to shared
+// memory, the horizontal transfer in closed form (binomial sums, the same transfer
+// as eri_device.cuh) gives first (ab|f0] and then (ab|cd), which is normalized and
+// digested by the lanes into the six Fock blocks (lane-owned sums, no shared-memory
+// atomics).  J'_ab accumulates in shared memory while consecutive quartets of the
+// warp keep their bra pair and goes to global memory once per bra pair; the other
+// five blocks take one global atomic per element and quartet.
+//
+// Compared with the tiled kernel, the transfer runs once per contracted quartet
+// instead of once per primitive quartet and root, the per-primitive work is
+// compile-time unrolled, and the contraction needs three shared-memory loads per
+// (e0|f0) integral and root.  The reference counterparts are the same as the tiled
+// kernel's (src/device/cuda/kernels/eri_kernel_warp.cu:140-344 plus the separate
+// fock_accumulate_batch_kernel).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "eri_device.cuh"
+#include "eri_kernels.h"
+
+namespace lai {
+
+constexpr int kWarpqMaxG = 1152;    // (e0|f0) integrals per quartet: 36 per lane
+constexpr int kWarpqWarps = 4;      // warps per block
+
+__host__ __device__ constexpr int warpq_max(int a, int b) { return a > b ? a : b; }
+
+template <int LA, int LB, int LC, int LD>
+struct WarpqClass {
+  static constexpr int LAB = LA + LB, LCD = LC + LD;
+  static constexpr int NR = (LAB + LCD) / 2 + 1;
+  static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  static constexpr int NE = ncart_range(LA, LAB), NF = ncart_range(LC, LCD);
+  static constexpr int NG = NE * NF, MG = (NG + 31) / 32;
+  static constexpr int W = LCD + 1, VS = (LAB + 1) * W;
+  static constexpr int NAB = NA * NB, NCD = NC * ND;
+  static constexpr int NX = NAB * NF, NO = NAB * NCD;
+  static constexpr int NACC = NAB + NCD + NA * NC + NA * ND + NB * NC + NB * ND;
+  // per-warp shared memory (doubles): root tables, two block buffers, density
+  // sub-blocks, the running J'_ab of the current bra pair
+  static constexpr int S_V = NR * 3 * VS;
+  static constexpr int S_BUF = warpq_max(NG, warpq_max(NX, NO));
+  static constexpr int OFF_B0 = S_V, OFF_B1 = OFF_B0 + S_BUF, OFF_D = OFF_B1 + S_BUF;
+  static constexpr int OFF_JAB = OFF_D + NACC;
+  static constexpr int PER_WARP = ((OFF_JAB + NAB) + 1) & ~1;
+  // blocks per SM the register allocation targets: the warp's latency (dependent
+  // global loads, warp syncs) is hidden by other warps, so the small classes are
+  // held to few registers (estimate: G, its offsets, one lane's 2D table, ~40 more)
+  static constexpr int REG_EST = 3 * MG + 2 * VS + 40;
+  static constexpr int MIN_BLOCKS = REG_EST <= 64 ? 8 : REG_EST <= 80 ? 6 : REG_EST <= 96 ? 5
+                                    : REG_EST <= 128 ? 4 : REG_EST <= 168 ? 3 : 2;
+};
+
+// The CUDA error of the last failed launch (cudaGetLastError clears it).
+inline cudaError_t& warpq_last_error() {
+  static thread_local cudaError_t e = cudaSuccess;
+  return e;
+}
+
+__device__ __forceinline__ int warpq_binom(int n, int k) {
+  int r = 1;
+  for (int i = 0; i < k; ++i) r = r * (n - i) / (i + 1);
+  return r;
+}
+
+__device__ __forceinline__ double warpq_pow(double x, int m) {
+  double r = 1.0;
+  for (int i = 0; i < m; ++i) r *= x;
+  return r;
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>::MIN_BLOCKS)) eri_warpq_kernel(QuartetBlock blk, JKArgs args,
+                                                                     RysTablesView tab) {
+  using C = WarpqClass<LA, LB, LC, LD>;
+  constexpr int NR = C::NR, W = C::W, VS = C::VS, MG = C::MG, NF = C::NF;
+  constexpr int NA = C::NA, NB = C::NB, NC = C::NC, ND = C::ND, NCD = C::NCD, NAB = C::NAB;
+  constexpr int LAB = C::LAB, LCD = C::LCD;
+  extern __shared__ __align__(16) double smem_q[];
+  // Cartesian components (packed lx | ly << 4 | lz << 8) and normalization factors
+  // of the four shells
+  __shared__ int s_comp[4][kNCartMax];
+  __shared__ double s_norm[4][kNCartMax];
+  for (int i = threadIdx.x; i < 4 * kNCartMax; i += blockDim.x) {
+    const int sh = i / kNCartMax, k = i - sh * kNCartMax;
+    const int l = sh == 0 ? LA : sh == 1 ? LB : sh == 2 ? LC : LD;
+    if (k < ncart(l)) {
+      s_comp[sh][k] = cart_comp(l, k);
+      s_norm[sh][k] = norm_factor(l, k);
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  double* const Vs = smem_q + (size_t)warp * C::PER_WARP;
+  double* const B0 = Vs + C::OFF_B0;
+  double* const B1 = Vs + C::OFF_B1;
+  double* const Ds = Vs + C::OFF_D;
+  double* const Jab = Vs + C::OFF_JAB;
+  constexpr int oDab = 0, oDcd = NAB, oDac = oDcd + NCD, oDad = oDac + NA * NC, oDbc = oDad + NA * ND,
+                oDbd = oDbc + NB * NC;
+
+  // this lane's (e0|f0) integrals: packed byte offsets of Ix, Iy, Iz inside one
+  // direction's table (10 bits each); entries past the block read I(0,0) and are
+  // never written out
+  int goff[MG];
+#pragma unroll
+  for (int m = 0; m < MG; ++m) {
+    const int j = lane + 32 * m;
+    int o = 0;
+    if (j < C::NG) {
+      const int e = j / NF, f = j - e * NF;
+      int le = LA, re = e;
+      while (re >= ncart(le)) re -= ncart(le++);
+      int lf = LC, rf = f;
+      while (rf >= ncart(lf)) rf -= ncart(lf++);
+      const int ce = cart_comp(le, re), cf = cart_comp(lf, rf);
+      const int ox = comp_x(ce) * W + comp_x(cf), oy = comp_y(ce) * W + comp_y(cf),
+                oz = comp_z(ce) * W + comp_z(cf);
+      o = (ox * 8) | ((oy * 8) << 10) | ((oz * 8) << 20);
+    }
+    goff[m] = o;
+  }
+
+  const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
+  const int Kab = blk.bra.Ka * blk.bra.Kb, Kcd = blk.ket.Ka * blk.ket.Kb;
+  const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
+
+  const int64_t gw = (int64_t)blockIdx.x * kWarpqWarps + warp;
+  const int64_t nw = (int64_t)gridDim.x * kWarpqWarps;
+  const int64_t nq_all = blk.total - blk.t_begin;
+  const int64_t per = (nq_all + nw - 1) / nw;
+  const int64_t tbeg = blk.t_begin + gw * per;
+  const int64_t tend = min(blk.total, tbeg + per);
+  int p = -1;
+  int jab_p = -1;             // bra pair whose J'_ab is accumulating in Jab
+  int jab_fa = 0, jab_fb = 0;
+  double* jab_J = nullptr;
+  size_t jab_n = 0;
+  unsigned int nprim_done = 0;
+  for (int i = lane; i < NAB; i += 32) Jab[i] = 0.0;
+
+  for (int64_t t = tbeg; t < tend; ++t) {
+    if (p < 0) {
+      if (lane == 0) p = find_bra(blk.offsets, nbra, t);
+      p = __shfl_sync(0xffffffffu, p, 0);
+    } else {
+      while (t >= __ldg(blk.offsets + p + 1)) ++p;
+    }
+    const int q = (blk.qbegin ? __ldg(blk.qbegin + p) : 0) + (int)(t - __ldg(blk.offsets + p));
+    const int fa = __ldg(blk.bra.func_a + p), fb = __ldg(blk.bra.func_b + p);
+    const int fc = __ldg(blk.ket.func_a + q), fd = __ldg(blk.ket.func_b + q);
+    const double sym = quartet_weight(blk, p, q);
+    const SysMats mats = sys_mats(args, blk, p);
+    const size_t n = (size_t)mats.nbf;
+    if (p != jab_p) {  // flush the finished bra pair's J'_ab
+      __syncwarp();
+      if (jab_p >= 0)
+        for (int i = lane; i < NAB; i += 32) {
+          const double v = Jab[i];
+          if (v != 0.0) atomicAdd(jab_J + (size_t)(jab_fa + i / NB) * jab_n + jab_fb + i % NB, v);
+          Jab[i] = 0.0;
+        }
+      jab_p = p;
+      jab_fa = fa;
+      jab_fb = fb;
+      jab_J = mats.J;
+      jab_n = n;
+    }
+    // density sub-blocks of the six scatter targets
+    for (int i = lane; i < C::NACC; i += 32) {
+      int r0, c0, c1, k;
+      if (i < oDcd) { k = i; r0 = fa; c0 = fb; c1 = NB; }
+      else if (i < oDac) { k = i - oDcd; r0 = fc; c0 = fd; c1 = ND; }
+      else if (i < oDad) { k = i - oDac; r0 = fa; c0 = fc; c1 = NC; }
+      else if (i < oDbc) { k = i - oDad; r0 = fa; c0 = fd; c1 = ND; }
+      else if (i < oDbd) { k = i - oDbc; r0 = fb; c0 = fc; c1 = NC; }
+      else { k = i - oDbd; r0 = fb; c0 = fd; c1 = ND; }
+      Ds[i] = __ldg(mats.D + (size_t)(r0 + k / c1) * n + c0 + k % c1);
+    }
+
+    double G[MG];
+#pragma unroll
+    for (int m = 0; m < MG; ++m) G[m] = 0.0;
+
+    for (int ib = 0; ib < Kab; ++ib) {
+      const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
+      const double qab = __ldg(pb + PF_Q * sb);
+      if (qab * blk.ket.qprim_max < args.prim_eps) break;
+      const double zeta = __ldg(pb + PF_ZETA * sb), hz = __ldg(pb + PF_HZ * sb);
+      const double Px = __ldg(pb + PF_PX * sb), Py = __ldg(pb + PF_PY * sb), Pz = __ldg(pb + PF_PZ * sb);
+      const double PAx = __ldg(pb + PF_PAX * sb), PAy = __ldg(pb + PF_PAY * sb), PAz = __ldg(pb + PF_PAZ * sb);
+      const double cab = __ldg(pb + PF_C * sb);
+      for (int ik = 0; ik < Kcd; ++ik) {
+        const double* pk = blk.ket.prim + (size_t)ik * nket + q;
+        const double qcd = __ldg(pk + PF_Q * sk);
+        if (qab * qcd < args.prim_eps) break;
+        ++nprim_done;
+        const double eta = __ldg(pk + PF_ZETA * sk), he = __ldg(pk + PF_HZ * sk);
+        const double PQx = Px - __ldg(pk + PF_PX * sk), PQy = Py - __ldg(pk + PF_PY * sk),
+                     PQz = Pz - __ldg(pk + PF_PZ * sk);
+        const double ccd = __ldg(pk + PF_C * sk);
+        const double rs = rsqrt(zeta + eta);
+        const double inv = rs * rs;
+        const double rz = eta * inv, re = zeta * inv;
+        const double T = zeta * rz * (PQx * PQx + PQy * PQy + PQz * PQz);
+        const double pref = cab * ccd * rs;
+        if (lane < 3 * NR) {
+          const int r = lane / 3, x = lane - 3 * r;
+          double u, w;
+          rys_root_one<double>(NR, r, T, tab, u, w);
+          const double pqx = x == 0 ? PQx : x == 1 ? PQy : PQz;
+          const double pax = x == 0 ? PAx : x == 1 ? PAy : PAz;
+          const double qcx = x == 0 ? __ldg(pk + PF_PAX * sk) : x == 1 ? __ldg(pk + PF_PAY * sk)
+                                                                    : __ldg(pk + PF_PAZ * sk);
+          const double pa = pax - rz * u * pqx;
+          const double qc = qcx + re * u * pqx;
+          const double b00 = 0.5 * inv * u, b10 = hz - hz * rz * u, b01 = he - he * re * u;
+          double V[LAB + 1][W];
+          V[0][0] = (x == 2) ? w * pref : 1.0;
+#pragma unroll
+          for (int e = 0; e < LAB; ++e)
+            V[e + 1][0] = pa * V[e][0] + (e ? double(e) * b10 * V[e > 0 ? e - 1 : 0][0] : 0.0);
+#pragma unroll
+          for (int f = 0; f < LCD; ++f)
+#pragma unroll
+            for (int e = 0; e <= LAB; ++e)
+              V[e][f + 1] = qc * V[e][f] + (f ? double(f) * b01 * V[e][f > 0 ? f - 1 : 0] : 0.0) +
+                            (e ? double(e) * b00 * V[e > 0 ? e - 1 : 0][f] : 0.0);
+          double* dst = Vs + (r * 3 + x) * VS;
+#pragma unroll
+          for (int e = 0; e <= LAB; ++e)
+#pragma unroll
+            for (int f = 0; f < W; ++f) dst[e * W + f] = V[e][f];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const char* vx = reinterpret_cast<const char*>(Vs + (r * 3) * VS);
+          const char* vy = vx + VS * 8;
+          const char* vz = vy + VS * 8;
+#pragma unroll
+          for (int m = 0; m < MG; ++m) {
+            const int o = goff[m];
+            G[m] += *reinterpret_cast<const double*>(vx + (o & 1023)) *
+                    *reinterpret_cast<const double*>(vy + ((o >> 10) & 1023)) *
+                    *reinterpret_cast<const double*>(vz + (o >> 20));
+          }
+        }
+        __syncwarp();
+      }
+    }
+
+    // ---- once per contracted quartet: transfer, normalization, digestion ----
+#pragma unroll
+    for (int m = 0; m < MG; ++m) {
+      const int j = lane + 32 * m;
+      if (j < C::NG) B0[j] = G[m];
+    }
+    const double ABx = __ldg(blk.bra.AB + p), ABy = __ldg(blk.bra.AB + nbra + p),
+                 ABz = __ldg(blk.bra.AB + 2 * nbra + p);
+    const double CDx = __ldg(blk.ket.AB + q), CDy = __ldg(blk.ket.AB + nket + q),
+                 CDz = __ldg(blk.ket.AB + 2 * nket + q);
+    __syncwarp();
+    // bra transfer: (ab|f0] = sum_k prod_x C(b_x, k_x) AB_x^(b_x - k_x) (a+k 0|f0]
+    for (int j = lane; j < C::NX; j += 32) {
+      const int ab = j / NF, f = j - ab * NF;
+      const int a = ab / NB, b = ab - a * NB;
+      const int ca = s_comp[0][a], cb = s_comp[1][b];
+      const int ax = comp_x(ca), ay = comp_y(ca), az = comp_z(ca);
+      const int bx = comp_x(cb), by = comp_y(cb), bz = comp_z(cb);
+      double s = 0.0;
+      for (int kx = 0; kx <= bx; ++kx) {
+        const double cx = warpq_binom(bx, kx) * warpq_pow(ABx, bx - kx);
+        for (int ky = 0; ky <= by; ++ky) {
+          const double cy = cx * warpq_binom(by, ky) * warpq_pow(ABy, by - ky);
+          for (int kz = 0; kz <= bz; ++kz) {
+            const int l = LA + kx + ky + kz;
+            const int e = ncart_before(LA, l) + cart_index(ax + kx, ay + ky, az + kz);
+            s += cy * warpq_binom(bz, kz) * warpq_pow(ABz, bz - kz) * B0[e * NF + f];
+          }
+        }
+      }
+      B1[j] = s;
+    }
+    __syncwarp();
+    // ket transfer and normalization: (ab|cd) into B0[ab][c][d]
+    for (int j = lane; j < C::NO; j += 32) {
+      const int ab = j / NCD, cd = j - ab * NCD;
+      const int c = cd / ND, d = cd - c * ND;
+      const int a = ab / NB, b = ab - a * NB;
+      const int cc = s_comp[2][c], cdc = s_comp[3][d];
+      const int cx0 = comp_x(cc), cy0 = comp_y(cc), cz0 = comp_z(cc);
+      const int dx = comp_x(cdc), dy = comp_y(cdc), dz = comp_z(cdc);
+      const double* row = B1 + ab * NF;
+      double s = 0.0;
+      for (int kx = 0; kx <= dx; ++kx) {
+        const double wx = warpq_binom(dx, kx) * warpq_pow(CDx, dx - kx);
+        for (int ky = 0; ky <= dy; ++ky) {
+          const double wy = wx * warpq_binom(dy, ky) * warpq_pow(CDy, dy - ky);
+          for (int kz = 0; kz <= dz; ++kz) {
+            const int l = LC + kx + ky + kz;
+            const int f = ncart_before(LC, l) + cart_index(cx0 + kx, cy0 + ky, cz0 + kz);
+            s += wy * warpq_binom(dz, kz) * warpq_pow(CDz, dz - kz) * row[f];
+          }
+        }
+      }
+      B0[j] = s * s_norm[0][a] * s_norm[1][b] * s_norm[2][c] * s_norm[3][d];
+    }
+    __syncwarp();
+    // digestion: every lane owns whole Fock elements; J'_ab = 2s sum_cd V D_cd,
+    // J'_cd = 2s sum_ab V D_ab, K'_ac = s sum_bd V D_bd, K'_ad = s sum_bc V D_bc,
+    // K'_bc = s sum_ad V D_ad, K'_bd = s sum_ac V D_ac
+    const double* O = B0;
+    for (int i = lane; i < C::NACC; i += 32) {
+      double acc = 0.0;
+      if (i < oDcd) {
+        const double* row = O + i * NCD;
+#pragma unroll 4
+        for (int cd = 0; cd < NCD; ++cd) acc += row[cd] * Ds[oDcd + cd];
+        Jab[i] += 2.0 * sym * acc;
+        continue;
+      }
+      int r0, c0, c1, k;
+      double* M;
+      if (i < oDac) {
+        k = i - oDcd;
+#pragma unroll 4
+        for (int ab = 0; ab < NAB; ++ab) acc += O[ab * NCD + k] * Ds[oDab + ab];
+        acc *= 2.0 * sym;
+        r0 = fc; c0 = fd; c1 = ND; M = mats.J;
+      } else if (i < oDad) {
+        k = i - oDac;
+        const int a = k / NC, c = k - a * NC;
+        for (int b = 0; b < NB; ++b)
+          for (int d = 0; d < ND; ++d) acc += O[((a * NB + b) * NC + c) * ND + d] * Ds[oDbd + b * ND + d];
+        acc *= sym;
+        r0 = fa; c0 = fc; c1 = NC; M = mats.K;
+      } else if (i < oDbc) {
+        k = i - oDad;
+        const int a = k / ND, d = k - a * ND;
+        for (int b = 0; b < NB; ++b)
+          for (int c = 0; c < NC; ++c) acc += O[((a * NB + b) * NC + c) * ND + d] * Ds[oDbc + b * NC + c];
+        acc *= sym;
+        r0 = fa; c0 = fd; c1 = ND; M = mats.K;
+      } else if (i < oDbd) {
+        k = i - oDbc;
+        const int b = k / NC, c = k - b * NC;
+        for (int a = 0; a < NA; ++a)
+          for (int d = 0; d < ND; ++d) acc += O[((a * NB + b) * NC + c) * ND + d] * Ds[oDad + a * ND + d];
+        acc *= sym;
+        r0 = fb; c0 = fc; c1 = NC; M = mats.K;
+      } else {
+        k = i - oDbd;
+        const int b = k / ND, d = k - b * ND;
+        for (int a = 0; a < NA; ++a)
+          for (int c = 0; c < NC; ++c) acc += O[((a * NB + b) * NC + c) * ND + d] * Ds[oDac + a * NC + c];
+        acc *= sym;
+        r0 = fb; c0 = fd; c1 = ND; M = mats.K;
+      }
+      if (acc != 0.0) atomicAdd(M + (size_t)(r0 + k / c1) * n + c0 + k % c1, acc);
+    }
+    __syncwarp();
+  }
+  // the last bra pair's J'_ab
+  __syncwarp();
+  if (jab_p >= 0)
+    for (int i = lane; i < NAB; i += 32) {
+      const double v = Jab[i];
+      if (v != 0.0) atomicAdd(jab_J + (size_t)(jab_fa + i / NB) * jab_n + jab_fb + i % NB, v);
+    }
+  count_prims(args.prim_count, lane == 0 ? nprim_done : 0u);
+}
+
+// Host side: per-warp shared memory of class (la, lb, lc, ld), or -1 when the
+// class is not instantiated.
+template <int LA, int LB, int LC, int LD>
+int launch_warpq_cls(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
+                     cudaStream_t stream, int num_sms) {
+  using C = WarpqClass<LA, LB, LC, LD>;
+  const size_t smem = (size_t)C::PER_WARP * 8 * kWarpqWarps;
+  static int per_sm = -1;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(eri_warpq_kernel<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return -3;
+  if (per_sm < 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, eri_warpq_kernel<LA, LB, LC, LD>, kWarpqWarps * 32,
+                                                      smem) != cudaSuccess)
+      return -3;
+    if (b <= 0) return -1;  // does not fit: the tiled kernel takes the class
+    per_sm = b;
+  }
+  const int64_t want = (blk.total - blk.t_begin + kWarpqWarps - 1) / kWarpqWarps;
+  const int64_t cap = (int64_t)num_sms * per_sm;
+  const int grid = (int)std::min<int64_t>(want, cap);
+  eri_warpq_kernel<LA, LB, LC, LD><<<grid, kWarpqWarps * 32, smem, stream>>>(blk, args, tab);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    warpq_last_error() = e;
+    return -3;
+  }
+  return 0;
+}
+
+}  // namespace lai
