@@ -301,6 +301,22 @@ LAI_API int lai_sph_to_cart_density_device(lai_engine* engine, const double* d_D
  * _kernel.cpp).  charge_xyz [ncharge][3] (Bohr) and charge_q [ncharge] are host
  * arrays (NULL with ncharge = 0 for S and T).  Not available for batched engines.
  * ------------------------------------------------------------------------- */
+/* ---------------------------------------------------------------------------
+ * Density-fitting integrals.  aux: an auxiliary basis (any lai_basis, e.g. the
+ * reference's built-in cc-pVDZ-RI shells), normalized like an orbital basis.
+ *   lai_eri3c: T[(mu*nbf + nu)*naux + P] = (mu nu|P), both mu nu orders
+ *              (the reference's ThreeCenterStorageFormat::abP,
+ *              src/host/kernels/three_center_eri_kernel.cpp:273-362);
+ *   lai_eri2c: V[P*naux + Q] = (P|Q) (compute_two_center_metric,
+ *              src/host/kernels/two_center_coulomb_kernel.cpp:212-251).
+ * Orbital shells up to f (g only paired with s), auxiliary shells up to g.  The
+ * _device variants write device buffers asynchronously on stream.
+ * ------------------------------------------------------------------------- */
+LAI_API int lai_eri3c(lai_engine* engine, const lai_basis* aux, double* T);
+LAI_API int lai_eri2c(lai_engine* engine, const lai_basis* aux, double* V);
+LAI_API int lai_eri3c_device(lai_engine* engine, const lai_basis* aux, double* d_T, void* stream);
+LAI_API int lai_eri2c_device(lai_engine* engine, const lai_basis* aux, double* d_V, void* stream);
+
 #define LAI_OP_OVERLAP 0
 #define LAI_OP_KINETIC 1
 #define LAI_OP_NUCLEAR 2

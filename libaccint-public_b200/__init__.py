@@ -7,4 +7,4 @@ from ._lib import LibAccIntError, lib  # noqa: F401
 from .basis import Atom, BasisSet, Shell, basis_data, cart_to_sph_matrix, point_charges  # noqa: F401
 from .engine import (BatchedEngine, Engine, FockBuilder, Operator, ScreeningOptions, jk,  # noqa: F401
                      probe_fp64_peak)
-from . import autograd, molecules, scf, workloads  # noqa: F401
+from . import autograd, df, molecules, scf, workloads  # noqa: F401

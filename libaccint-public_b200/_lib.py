@@ -29,6 +29,7 @@ EXPORTED = [
     "lai_engine_create_batched", "lai_engine_batch_layout", "lai_jk_build_batched",
     "lai_engine_autotune", "lai_shard_range", "lai_engine_tune_table",
     "lai_one_electron", "lai_one_electron_device", "lai_basis_from_bse_json",
+    "lai_eri3c", "lai_eri2c", "lai_eri3c_device", "lai_eri2c_device",
 ]
 
 LAI_OP_OVERLAP, LAI_OP_KINETIC, LAI_OP_NUCLEAR, LAI_OP_HCORE = 0, 1, 2, 3
@@ -120,6 +121,10 @@ def lib():
         "lai_one_electron": (I, [P, I, I, P, P, P]),
         "lai_one_electron_device": (I, [P, I, I, P, P, P, P]),
         "lai_basis_from_bse_json": (I, [ctypes.c_char_p, ctypes.c_size_t, I, P, P, ctypes.POINTER(P)]),
+        "lai_eri3c": (I, [P, P, P]),
+        "lai_eri2c": (I, [P, P, P]),
+        "lai_eri3c_device": (I, [P, P, P, P]),
+        "lai_eri2c_device": (I, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

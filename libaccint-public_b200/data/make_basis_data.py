@@ -12,7 +12,9 @@ single-l BSE shell becomes its own contracted shell over ALL listed exponents
 (zero coefficients included), all-zero columns are skipped, and multi-l (SP)
 shells give one shell per l.  The built-in STO-3G (src/shared/data/builtin_basis.cpp)
 is parsed from its C++ literals: per element, a list of (l, exponents,
-coefficients) in emission order.  Coefficients are the raw, un-normalized
+coefficients) in emission order.  So are the reference's built-in auxiliary
+(density-fitting) sets of src/shared/data/auxiliary_basis_data.cpp (cc-pVDZ-RI,
+cc-pVTZ-RI, def2-SVP-JKFIT, def2-TZVP-JKFIT), stored under their lower-case names.  Coefficients are the raw, un-normalized
 contraction coefficients; normalization happens when a basis is built.
 """
 import json
@@ -57,6 +59,22 @@ def parse_builtin_sto3g(path):
     return out
 
 
+def parse_builtin_aux(path):
+    src = open(path).read()
+    names = {"hydrogen": "H", "carbon": "C", "nitrogen": "N", "oxygen": "O"}
+    sets = {"cc_pvdz_ri": "cc-pvdz-ri", "cc_pvtz_ri": "cc-pvtz-ri", "def2_svp_jkfit": "def2-svp-jkfit",
+            "def2_tzvp_jkfit": "def2-tzvp-jkfit"}
+    out = {v: {} for v in sets.values()}
+    for fn, body in re.findall(r"std::vector<AuxShellData> (\w+)\(\)\s*\{(.*?)\n\}", src, re.S):
+        for prefix, key in sets.items():
+            if fn.startswith(prefix + "_") and fn[len(prefix) + 1:] in names:
+                shells = []
+                for am, e, c in re.findall(r"\{\s*(\d+),\s*\{([^}]*)\},\s*\{([^}]*)\}\s*\}", body):
+                    shells.append([int(am), [float(x) for x in e.split(",")], [float(x) for x in c.split(",")]])
+                out[key][names[fn[len(prefix) + 1:]]] = shells
+    return out
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     data = {}
@@ -66,10 +84,11 @@ def main():
                       for z, sym in ELEMENTS.items() if z in j["elements"]}
     data["sto-3g-builtin"] = parse_builtin_sto3g(
         os.path.join(ref, "src", "shared", "data", "builtin_basis.cpp"))
+    data.update(parse_builtin_aux(os.path.join(ref, "src", "shared", "data", "auxiliary_basis_data.cpp")))
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "basis_sets.json"), "w") as f:
         json.dump({"source": "reference share/basis_sets (Basis Set Exchange) and "
-                             "src/shared/data/builtin_basis.cpp",
+                             "src/shared/data/builtin_basis.cpp and auxiliary_basis_data.cpp",
                    "basis_sets": data}, f, separators=(",", ":"))
 
 

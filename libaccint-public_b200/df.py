@@ -1,0 +1,139 @@
+"""Density-fitted J and K on the device.
+
+    df = DFFockBuilder(engine, aux_basis)          # engine over the orbital basis
+    df.set_density(D)                              # (nbf, nbf), host array or cuda tensor
+    J, K = df.compute_coulomb(), df.compute_exchange()
+
+Mirrors consumers::DFFockBuilder (include/libaccint/consumers/df_fock_builder.hpp:
+99-200, src/shared/consumers/df_fock_builder.cpp): Coulomb metric V_PQ = (P|Q),
+V = L L^T, B_ab^P = sum_Q (ab|Q) (L^-1)_PQ, so that sum_P B_ab^P B_cd^P =
+(ab|Q) V^-1 (Q|cd) is the fitted (ab|cd);
+    J_ab = sum_P B_ab^P gamma_P,   gamma_P = sum_cd B_cd^P D_cd,
+    K_ac = sum_P sum_bd B_ab^P D_bd B_cd^P.
+Three- and two-centre integrals come from the device kernels of
+libaccint_b200.so (lai_eri3c_device / lai_eri2c_device); the metric
+factorization, the triangular solve and the contractions are FP64 cuBLAS /
+cuSOLVER calls through torch on tensors resident in HBM: K runs as one batched
+GEMM over the auxiliary index after factoring D = C+ C+^T - C- C-^T (symmetric
+eigendecomposition), and one large GEMM.
+
+The reference forms B = T L^-1 (three_center_eri_kernel.cpp:364-387 with L_inv from
+math::triangular_inverse), which is the fitted (ab|cd) only if L^T L = L L^T; and
+its two-centre metric is not positive definite for the built-in cc-pVDZ-RI set
+(its own DF tests skip on the resulting exception).  The fitting here is the
+textbook one; it is checked against an independent restatement of the integrals
+and against the exact four-centre J/K it approximates.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class DFFockBuilder:
+    def __init__(self, engine, aux, metric="coulomb", exchange_fraction=0.5, eig_cut=1e-14):
+        if metric != "coulomb":
+            raise ValueError(f"metric {metric!r} is not supported (Coulomb metric only)")
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("DFFockBuilder runs on a CUDA device; none is available")
+        self.engine = engine
+        self.aux = aux
+        self.n = engine.basis.nbf
+        self.naux = aux.nbf
+        self.exchange_fraction = exchange_fraction
+        self.eig_cut = eig_cut
+        self.dev = torch.device("cuda", engine.device)
+        self.BT = None        # (naux, n, n): B^P matrices, contiguous per P
+        self.D = None
+        self.J = None
+        self.K = None
+        self.init_ms = None
+
+    def initialize(self):
+        """Metric, its Cholesky factor and the fitted three-centre tensor."""
+        if self.BT is not None:
+            return
+        torch = _torch()
+        n, naux = self.n, self.naux
+        with torch.cuda.device(self.dev):
+            s = torch.cuda.current_stream(self.dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            V = torch.empty((naux, naux), dtype=torch.float64, device=self.dev)
+            _lib.check(_lib.lib().lai_eri2c_device(self.engine._h, self.aux.handle(), ctypes.c_void_p(V.data_ptr()),
+                                                   ctypes.c_void_p(s.cuda_stream)))
+            V = 0.5 * (V + V.T)
+            L = torch.linalg.cholesky(V)
+            T = torch.empty((n * n, naux), dtype=torch.float64, device=self.dev)
+            _lib.check(_lib.lib().lai_eri3c_device(self.engine._h, self.aux.handle(),
+                                                   ctypes.c_void_p(T.data_ptr()), ctypes.c_void_p(s.cuda_stream)))
+            # B^T = L^-1 T^T  (naux x n^2)
+            self.BT = torch.linalg.solve_triangular(L, T.T, upper=False).reshape(naux, n, n).contiguous()
+            del T
+            e1.record(s)
+            e1.synchronize()
+            self.init_ms = e0.elapsed_time(e1)
+
+    def set_density(self, D, nbf=None):
+        torch = _torch()
+        if nbf is not None and nbf != self.n:
+            raise ValueError("DFFockBuilder::set_density: nbf mismatch")
+        Dt = torch.as_tensor(D, dtype=torch.float64).to(self.dev)
+        if Dt.shape != (self.n, self.n):
+            raise ValueError(f"density must be {self.n}x{self.n}")
+        self.D = Dt
+
+    def _need(self):
+        if self.D is None:
+            raise RuntimeError("DFFockBuilder: density matrix not set")
+        self.initialize()
+
+    def compute_coulomb(self):
+        self._need()
+        n, naux = self.n, self.naux
+        B2 = self.BT.reshape(naux, n * n)
+        gamma = B2 @ self.D.reshape(-1)
+        self.J = (B2.T @ gamma).reshape(n, n)
+        return self.J
+
+    def compute_exchange(self):
+        self._need()
+        torch = _torch()
+        n, naux = self.n, self.naux
+        Ds = 0.5 * (self.D + self.D.T)
+        lam, U = torch.linalg.eigh(Ds)
+        scale = torch.max(torch.abs(lam)) if lam.numel() else torch.tensor(0.0)
+        K = torch.zeros((n, n), dtype=torch.float64, device=self.dev)
+        for sign in (1.0, -1.0):
+            keep = sign * lam > self.eig_cut * scale
+            if not bool(torch.any(keep)):
+                continue
+            C = U[:, keep] * torch.sqrt(sign * lam[keep])
+            X = torch.matmul(self.BT, C)                       # (naux, n, m)
+            Xf = X.permute(1, 0, 2).reshape(n, -1)             # (n, naux*m)
+            K = K + sign * (Xf @ Xf.T)
+        self.K = K
+        return K
+
+    def compute(self):
+        """F_2e = J - exchange_fraction K (DFFockBuilder::compute)."""
+        J = self.compute_coulomb()
+        K = self.compute_exchange()
+        return J - self.exchange_fraction * K
+
+    def fock_matrix(self, H_core):
+        torch = _torch()
+        return torch.as_tensor(H_core, dtype=torch.float64).to(self.dev) + self.compute()
+
+    def get_coulomb_matrix(self):
+        return self.J
+
+    def get_exchange_matrix(self):
+        return self.K

@@ -92,6 +92,7 @@ class Engine:
         """``prim_threshold``: primitive-quartet cut (None = 1e-3 * threshold, 0 = off)."""
         self.basis = basis
         self.threshold = threshold
+        self.device = device
         L = _lib.lib()
         opts = _lib.EngineOpts()
         L.lai_engine_opts_default(ctypes.byref(opts))

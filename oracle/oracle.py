@@ -48,6 +48,8 @@ def restatement():
         L.orc_jk_sym.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _D]
         L.orc_jk_sym.restype = ctypes.c_long
         L.orc_one_electron.argtypes = [_I, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P]
+        L.orc_eri3c.argtypes = [_I, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]
+        L.orc_eri2c.argtypes = [_I, _P, _P, _P, _P, _P, _P]
         _orc = L
     return _orc
 
@@ -86,6 +88,17 @@ def reference():
         L.ref_cart_to_sph.argtypes = [_I, _P]
         L.ref_one_electron.restype = _I
         L.ref_one_electron.argtypes = [_P, _I, _I, _P, _P, _P]
+        L.ref_aux_builtin.restype = _P
+        L.ref_aux_builtin.argtypes = [ctypes.c_char_p, _I, _P, _P]
+        L.ref_aux_free.argtypes = [_P]
+        L.ref_aux_nbf.restype = _L
+        L.ref_aux_nbf.argtypes = [_P]
+        L.ref_aux_nshell.restype = _L
+        L.ref_aux_nshell.argtypes = [_P]
+        L.ref_aux_shell.argtypes = [_P, _L, _P, _P, _P, _P, _P]
+        L.ref_eri3c.argtypes = [_P, _P, _P]
+        L.ref_eri2c.argtypes = [_P, _P]
+        L.ref_df_jk.argtypes = [_P, _P, _P, _P, _P]
         _ref = L
     return _ref
 
@@ -199,6 +212,29 @@ def orc_one_electron(basis, kind, xyz=None, q=None):
     if rc != 0:
         raise RuntimeError("orc_one_electron failed")
     return out
+
+
+def orc_eri3c(basis, aux):
+    """T[a][b][P] = (ab|P) by the restatement (orc_eri_quartet with a unit s shell)."""
+    O = restatement()
+    l, nprim, centers, exps, coefs = normalized_arrays(basis)
+    lx, npx, cx, ex, cfx = normalized_arrays(aux)
+    T = np.zeros((basis.nbf, basis.nbf, aux.nbf))
+    rc = O.orc_eri3c(len(l), l.ctypes.data, nprim.ctypes.data, centers.ctypes.data, exps.ctypes.data,
+                     coefs.ctypes.data, len(lx), lx.ctypes.data, npx.ctypes.data, cx.ctypes.data,
+                     ex.ctypes.data, cfx.ctypes.data, T.ctypes.data)
+    assert rc == 0
+    return T
+
+
+def orc_eri2c(aux):
+    """V[P][Q] = (P|Q) by the restatement."""
+    O = restatement()
+    lx, npx, cx, ex, cfx = normalized_arrays(aux)
+    V = np.zeros((aux.nbf, aux.nbf))
+    assert O.orc_eri2c(len(lx), lx.ctypes.data, npx.ctypes.data, cx.ctypes.data, ex.ctypes.data,
+                       cfx.ctypes.data, V.ctypes.data) == 0
+    return V
 
 
 def nuclear_repulsion(Z, xyz):
@@ -391,6 +427,78 @@ class RefBasis:
         if getattr(self, "h", None):
             self.R.ref_basis_free(self.h)
             self.h = None
+
+
+class RefAux:
+    """The reference's built-in auxiliary basis (data::create_builtin_auxiliary_basis)."""
+
+    def __init__(self, name, Z, xyz):
+        R = reference()
+        if R is None:
+            raise RuntimeError("oracle/_ref/libref_oracle.so not built")
+        self.R = R
+        Z = np.ascontiguousarray(Z, dtype=np.int32)
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        self.h = R.ref_aux_builtin(name.encode(), len(Z), Z.ctypes.data, xyz.ctypes.data)
+        if not self.h:
+            raise RuntimeError(R.ref_last_error().decode())
+        self.nbf = R.ref_aux_nbf(self.h)
+        self.nshell = R.ref_aux_nshell(self.h)
+
+    def shells(self):
+        """[(l, center, exps, normalized coefs)]"""
+        out = []
+        for i in range(self.nshell):
+            l, k = ctypes.c_int(), ctypes.c_int()
+            c = np.zeros(3)
+            self.R.ref_aux_shell(self.h, i, ctypes.byref(l), ctypes.byref(k), c.ctypes.data, None, None)
+            e, cf = np.zeros(k.value), np.zeros(k.value)
+            self.R.ref_aux_shell(self.h, i, ctypes.byref(l), ctypes.byref(k), c.ctypes.data, e.ctypes.data,
+                                 cf.ctypes.data)
+            out.append((l.value, c, e, cf))
+        return out
+
+    def eri3c(self, ref_basis):
+        T = np.zeros((ref_basis.nbf, ref_basis.nbf, self.nbf))
+        assert self.R.ref_eri3c(ref_basis.h, self.h, T.ctypes.data) == 0, self.R.ref_last_error().decode()
+        return T
+
+    def eri2c(self):
+        V = np.zeros((self.nbf, self.nbf))
+        assert self.R.ref_eri2c(self.h, V.ctypes.data) == 0, self.R.ref_last_error().decode()
+        return V
+
+    def df_jk(self, ref_basis, D):
+        n = ref_basis.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        rc = self.R.ref_df_jk(ref_basis.h, self.h, D.ctypes.data, J.ctypes.data, K.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(self.R.ref_last_error().decode())
+        return J, K
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.R.ref_aux_free(self.h)
+            self.h = None
+
+
+def df_jk_from_integrals(T, V, D, convention="exact"):
+    """J and K of density fitting from three-centre T[a][b][P] and metric V[P][Q]
+    (numpy, test infrastructure).  exact: B = T L^-T with V = L L^T, so B B^T =
+    T V^-1 T^T.  reference: B = T L^-1, the B tensor of the reference's
+    DFFockBuilder::compute_b_tensor (src/host/kernels/three_center_eri_kernel.cpp:
+    364-387 with L_inv from math::triangular_inverse)."""
+    n, naux = T.shape[0], T.shape[2]
+    L = np.linalg.cholesky(V)
+    Li = np.linalg.inv(L)
+    Tm = T.reshape(n * n, naux)
+    B = Tm @ (Li.T if convention == "exact" else Li)
+    gamma = B.T @ D.reshape(-1)
+    J = (B @ gamma).reshape(n, n)
+    Bp = B.reshape(n, n, naux)
+    K = np.einsum("abP,bd,cdP->ac", Bp, D, Bp)
+    return J, K
 
 
 class CanonicalQuartets:

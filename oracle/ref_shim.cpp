@@ -20,6 +20,11 @@
 //   - math::get_cart_to_sph_matrix            include/libaccint/math/spherical_transform.hpp:20-40
 //   - Engine::compute_overlap_matrix / compute_kinetic_matrix / compute_nuclear_matrix
 //                                             include/libaccint/engine/engine.hpp:831-900
+//   - data::create_builtin_auxiliary_basis    src/shared/data/auxiliary_basis_data.cpp:735-776
+//   - kernels::compute_three_center_tensor (abP) / compute_two_center_metric
+//                                             src/host/kernels/three_center_eri_kernel.cpp:273-362,
+//                                             src/host/kernels/two_center_coulomb_kernel.cpp:212-251
+//   - consumers::DFFockBuilder                src/shared/consumers/df_fock_builder.cpp:102-450
 #include <libaccint/libaccint.hpp>
 #include <libaccint/engine/engine.hpp>
 #include <libaccint/consumers/fock_builder.hpp>
@@ -30,6 +35,11 @@
 #include <libaccint/math/spherical_transform.hpp>
 #include <libaccint/screening/schwarz_bounds.hpp>
 #include <libaccint/screening/screening_options.hpp>
+#include <libaccint/basis/auxiliary_basis_set.hpp>
+#include <libaccint/data/auxiliary_basis_data.hpp>
+#include <libaccint/consumers/df_fock_builder.hpp>
+#include <libaccint/kernels/three_center_eri_kernel.hpp>
+#include <libaccint/kernels/two_center_coulomb_kernel.hpp>
 
 #include <omp.h>
 
@@ -342,6 +352,80 @@ int ref_one_electron(void* h, int kind, int ncharge, const double* xyz, const do
         }
         if (r.size() != n * n) { set_err("ref_one_electron: unexpected result size"); return -1; }
         std::memcpy(out, r.data(), sizeof(double) * n * n);
+        return 0;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1;
+    }
+}
+
+// Built-in auxiliary basis (e.g. "cc-pVDZ-RI") on the atoms; NULL on error.
+void* ref_aux_builtin(const char* name, int natom, const int* Z, const double* xyz) {
+    try {
+        std::vector<data::Atom> atoms;
+        for (int a = 0; a < natom; ++a)
+            atoms.push_back({Z[a], Point3D(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2])});
+        return new AuxiliaryBasisSet(data::create_builtin_auxiliary_basis(name, atoms));
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return nullptr;
+    }
+}
+
+void ref_aux_free(void* h) { delete static_cast<AuxiliaryBasisSet*>(h); }
+long ref_aux_nbf(void* h) { return (long)static_cast<AuxiliaryBasisSet*>(h)->n_functions(); }
+long ref_aux_nshell(void* h) { return (long)static_cast<AuxiliaryBasisSet*>(h)->shells().size(); }
+
+// One auxiliary shell: am, nprim, center, exponents, NORMALIZED coefficients.
+int ref_aux_shell(void* h, long i, int* am, int* nprim, double* center, double* exps, double* coefs) {
+    const auto& sh = static_cast<AuxiliaryBasisSet*>(h)->shells()[(Size)i];
+    *am = sh.angular_momentum();
+    *nprim = (int)sh.n_primitives();
+    center[0] = sh.center().x;
+    center[1] = sh.center().y;
+    center[2] = sh.center().z;
+    if (exps) for (Size p = 0; p < sh.n_primitives(); ++p) exps[p] = sh.exponents()[p];
+    if (coefs) for (Size p = 0; p < sh.n_primitives(); ++p) coefs[p] = sh.coefficients()[p];
+    return 0;
+}
+
+// T[(a*n + b)*naux + P] = (ab|P) and V[P*naux + Q] = (P|Q) of the reference kernels.
+int ref_eri3c(void* hb, void* ha, double* T) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(hb)->basis;
+        auto& aux = *static_cast<AuxiliaryBasisSet*>(ha);
+        kernels::compute_three_center_tensor(basis.shells(), aux.shells(), T, basis.n_basis_functions(),
+                                             aux.n_functions(), kernels::ThreeCenterStorageFormat::abP);
+        return 0;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1;
+    }
+}
+
+int ref_eri2c(void* ha, double* V) {
+    try {
+        auto& aux = *static_cast<AuxiliaryBasisSet*>(ha);
+        kernels::compute_two_center_metric(aux.shells(), V, aux.n_functions());
+        return 0;
+    } catch (const std::exception& ex) {
+        set_err(ex.what());
+        return -1;
+    }
+}
+
+// DFFockBuilder(orbital, aux): set_density(D), compute_coulomb(), compute_exchange().
+int ref_df_jk(void* hb, void* ha, const double* D, double* J, double* K) {
+    try {
+        auto& basis = *static_cast<RefBasis*>(hb)->basis;
+        auto& aux = *static_cast<AuxiliaryBasisSet*>(ha);
+        const Size n = basis.n_basis_functions();
+        consumers::DFFockBuilder df(basis, aux);
+        df.set_density(std::span<const Real>(D, n * n));
+        const auto j = df.compute_coulomb();
+        const auto k = df.compute_exchange();
+        std::memcpy(J, j.data(), sizeof(double) * n * n);
+        std::memcpy(K, k.data(), sizeof(double) * n * n);
         return 0;
     } catch (const std::exception& ex) {
         set_err(ex.what());

@@ -646,3 +646,81 @@ int orc_one_electron(int n, const int *l, const int *nprim, const double *ctr, c
     basis_free(&b);
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Density-fitting integrals through orc_eri_quartet with a unit s function   */
+/* (exponent 0, coefficient 1) as the fourth shell: (ab|P) = (ab|P u),        */
+/* (P|Q) = (P u|Q u).  Orbital shells (no, lo, npo, co_, eo, cfo) and         */
+/* auxiliary shells (nx, ...) with normalized coefficients.                    */
+/*   T[(a*nbf + b)*naux + P] (both a b orders), V[P*naux + Q].                */
+/* Reference: compute_three_center_tensor (abP) and compute_two_center_metric */
+/* (src/host/kernels/three_center_eri_kernel.cpp:273-362,                      */
+/*  src/host/kernels/two_center_coulomb_kernel.cpp:212-251).                  */
+/* ------------------------------------------------------------------------- */
+static const double ORC_ZERO = 0.0, ORC_ONE = 1.0;
+
+int orc_eri3c(int no, const int *lo, const int *npo, const double *co, const double *eo, const double *cfo,
+              int nx, const int *lx, const int *npx, const double *cx, const double *ex, const double *cfx,
+              double *T) {
+    basis_t bo, bx;
+    basis_init(&bo, no, lo, npo, co, eo, cfo);
+    basis_init(&bx, nx, lx, npx, cx, ex, cfx);
+    const long nbf = bo.foff[no], naux = bx.foff[nx];
+    double *blk = malloc(sizeof(double) * 28 * 28 * 28);
+    int rc = 0;
+    for (int a = 0; a < no && !rc; ++a)
+        for (int b = a; b < no && !rc; ++b)
+            for (int p = 0; p < nx && !rc; ++p) {
+                const int l[4] = {lo[a], lo[b], lx[p], 0};
+                const int np[4] = {npo[a], npo[b], npx[p], 1};
+                double ctr[12];
+                memcpy(ctr, co + 3 * a, 24); memcpy(ctr + 3, co + 3 * b, 24);
+                memcpy(ctr + 6, cx + 3 * p, 24); memcpy(ctr + 9, cx + 3 * p, 24);
+                const double *e[4] = {eo + bo.poff[a], eo + bo.poff[b], ex + bx.poff[p], &ORC_ZERO};
+                const double *c[4] = {cfo + bo.poff[a], cfo + bo.poff[b], cfx + bx.poff[p], &ORC_ONE};
+                rc = orc_eri_quartet(l, ctr, np, e, c, blk);
+                const int na = ncart(l[0]), nb = ncart(l[1]), nq = ncart(l[2]);
+                for (int i = 0; i < na; ++i)
+                    for (int j = 0; j < nb; ++j)
+                        for (int k = 0; k < nq; ++k) {
+                            const double v = blk[(i * nb + j) * nq + k];
+                            const long ia = bo.foff[a] + i, jb = bo.foff[b] + j, kp = bx.foff[p] + k;
+                            T[(ia * nbf + jb) * naux + kp] = v;
+                            T[(jb * nbf + ia) * naux + kp] = v;
+                        }
+            }
+    free(blk);
+    basis_free(&bo);
+    basis_free(&bx);
+    return rc;
+}
+
+int orc_eri2c(int nx, const int *lx, const int *npx, const double *cx, const double *ex, const double *cfx,
+              double *V) {
+    basis_t bx;
+    basis_init(&bx, nx, lx, npx, cx, ex, cfx);
+    const long naux = bx.foff[nx];
+    double *blk = malloc(sizeof(double) * 28 * 28);
+    int rc = 0;
+    for (int p = 0; p < nx && !rc; ++p)
+        for (int q = p; q < nx && !rc; ++q) {
+            const int l[4] = {lx[p], 0, lx[q], 0};
+            const int np[4] = {npx[p], 1, npx[q], 1};
+            double ctr[12];
+            memcpy(ctr, cx + 3 * p, 24); memcpy(ctr + 3, cx + 3 * p, 24);
+            memcpy(ctr + 6, cx + 3 * q, 24); memcpy(ctr + 9, cx + 3 * q, 24);
+            const double *e[4] = {ex + bx.poff[p], &ORC_ZERO, ex + bx.poff[q], &ORC_ZERO};
+            const double *c[4] = {cfx + bx.poff[p], &ORC_ONE, cfx + bx.poff[q], &ORC_ONE};
+            rc = orc_eri_quartet(l, ctr, np, e, c, blk);
+            const int na = ncart(l[0]), nq = ncart(l[2]);
+            for (int i = 0; i < na; ++i)
+                for (int k = 0; k < nq; ++k) {
+                    const double v = blk[i * nq + k];
+                    V[(bx.foff[p] + i) * naux + bx.foff[q] + k] = v;
+                    V[(bx.foff[q] + k) * naux + bx.foff[p] + i] = v;
+                }
+        }
+    free(blk);
+    basis_free(&bx);
+    return rc;
+}
