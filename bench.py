@@ -14,6 +14,10 @@ and K (strong scaling, total work fixed).
 RHF calculation instead (one-electron integrals, the J/K build of every iteration,
 DIIS and diagonalization); its metric is seconds per converged SCF.
 
+``--workload df_<system>`` (e.g. df_h2o16_ccpvdz) times density-fitted J+K builds
+(auxiliary basis: the reference's built-in cc-pVDZ-RI) after the one-time metric and
+three-centre set-up; its metric is seconds per J+K build.
+
 ``--impl reference`` times the reference's own CPU implementation (the
 unmodified LibAccInt sources compiled into oracle/_ref: compute_2e_shell_quartet
 + FockBuilder::accumulate_symmetric, OpenMP over all host cores) on a seeded
@@ -158,7 +162,7 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    if args.workload.startswith("rhf_") or args.workload == "clusters256":
+    if args.workload.startswith(("rhf_", "df_")) or args.workload == "clusters256":
         print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the J/K build of a "
                           "single system; use --workload h2o64_ccpvdz (default)"}))
         return 0
@@ -363,6 +367,69 @@ def run_rhf(args):
     return 0
 
 
+def run_df(args):
+    """Density-fitted J+K builds (1 GPU; rank 0 only under torchrun)."""
+    import torch
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    lai = importlib.import_module("libaccint-public_b200")
+    name = args.workload[len("df_"):]
+    w = lai.workloads.make(name)
+    aux = lai.BasisSet.from_atoms(w.Z, w.xyz, "cc-pvdz-ri")
+    eng = lai.Engine(w.basis, threshold=w.thr, device=local)
+    df = lai.df.DFFockBuilder(eng, aux)
+    dev = torch.device("cuda", local)
+    D = torch.from_numpy(w.D).to(dev)
+    df.set_density(D)
+    df.initialize()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    s = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        df.compute_coulomb()
+        df.compute_exchange()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        J = df.compute_coulomb()
+        K = df.compute_exchange()
+        b.record(s)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    clk = clk.stop()
+    E = lai.molecules.energy(w.D, J.cpu().numpy(), K.cpu().numpy())
+    # the exact four-centre build of the same density, for the fitting error and the time
+    J4 = torch.empty_like(D)
+    K4 = torch.empty_like(D)
+    eng.jk_device(D.data_ptr(), J4.data_ptr(), K4.data_ptr(), stream=s.cuda_stream)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    eng.jk_device(D.data_ptr(), J4.data_ptr(), K4.data_ptr(), stream=s.cuda_stream)
+    b.record(s)
+    torch.cuda.synchronize()
+    E4 = lai.molecules.energy(w.D, J4.cpu().numpy(), K4.cpu().numpy())
+    out = {
+        "metric": "df_jk_seconds", "value": statistics.mean(ms) * 1e-3, "unit": "s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(ms),
+        "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "system": SYSTEMS.get(name, name), "nbf": w.nbf,
+                   "aux": "cc-pVDZ-RI (built-in set of the reference)", "naux": aux.nbf,
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "setup_ms": df.init_ms, "energy": E, "energy_four_center": E4, "fitting_error": E - E4,
+        "four_center_jk_ms": a.elapsed_time(b),
+        "clocks": clk,
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -371,6 +438,8 @@ def main():
         return run_batched(args)
     if args.workload.startswith("rhf_"):
         return run_rhf(args)
+    if args.workload.startswith("df_"):
+        return run_df(args)
     import torch
     import torch.distributed as dist
 

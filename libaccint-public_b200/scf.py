@@ -17,6 +17,9 @@ examples/mini-apps/python-hf/hf.py:239-372 runs the same iteration):
   the first iteration; the final energy comes from a fresh build at the
   converged density.
 
+With ``aux`` (an auxiliary BasisSet) J and K come from density fitting
+(df.DFFockBuilder) instead of the four-centre build.
+
 D, F, J, K, S, H and the DIIS history stay in device memory (torch float64
 tensors on the engine's device); only the energy, max |dD| and the DIIS
 B-matrix cross the bus each iteration.  The symmetric eigensolver is
@@ -66,7 +69,7 @@ class RHF:
     libaccint_b200.so).  ``fp32_cut`` enables the mixed-precision J/K build."""
 
     def __init__(self, basis, atoms=None, n_electrons=None, threshold=1e-12, device=0, fp32_cut=0.0,
-                 diis_size=6, engine=None):
+                 diis_size=6, engine=None, aux=None):
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("RHF runs on a CUDA device; none is available")
@@ -84,8 +87,18 @@ class RHF:
         self.fp32_cut = fp32_cut
         self.diis_size = diis_size
         self.e_nuc = nuclear_repulsion(self.atoms)
+        # density fitting: J/K from the auxiliary basis instead of the four-centre build
+        self.df = None
+        if aux is not None:
+            from .df import DFFockBuilder
+            self.df = DFFockBuilder(self.engine, aux)
 
     def _jk(self, D, J, K, stream):
+        if self.df is not None:
+            self.df.set_density(D)
+            J.copy_(self.df.compute_coulomb())
+            K.copy_(self.df.compute_exchange())
+            return
         self.engine.jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr(), stream=stream.cuda_stream,
                               fp32_cut=self.fp32_cut)
 
