@@ -148,13 +148,14 @@ def reference_sampler(w):
     return R, cq
 
 
-def time_reference(R, cq, D, target_s, seed):
-    """quartets/s of the reference CPU path on a uniform sample sized to ~target_s."""
-    n = 4000
-    t = R.time_quartets(D, cq.sample(n, seed), 0)[0]
+def time_reference(R, cq, D, target_s, seed, nthreads=0):
+    """quartets/s of the reference CPU path on a uniform sample sized to ~target_s
+    (nthreads 0 = all host cores)."""
+    n = 4000 if nthreads != 1 else 1000
+    t = R.time_quartets(D, cq.sample(n, seed), nthreads)[0]
     rate = n / max(t, 1e-6)
-    n = int(min(max(rate * target_s, 4000), 5e7))
-    t = R.time_quartets(D, cq.sample(n, seed + 1), 0)[0]
+    n = int(min(max(rate * target_s, 1000), 5e7))
+    t = R.time_quartets(D, cq.sample(n, seed + 1), nthreads)[0]
     return n / t, n, t
 
 
@@ -569,6 +570,11 @@ def main():
                        "sample": f"{ns} canonical quartets drawn uniformly (seeded) from the "
                                  f"{cq.total} of {args.workload}, {ts:.1f} s on all host cores; "
                                  f"full-build estimate {cq.total / rate:.0f} s"}
+                # the serial screened-symmetric path (one thread), the best correct
+                # single-core figure of the reference
+                r1, n1, t1 = time_reference(R, cq, w.D, max(2.0, args.cpu_seconds / 3), 11, nthreads=1)
+                cpu["value_1thread"] = r1
+                cpu["sample_1thread"] = f"{n1} canonical quartets, {t1:.1f} s on one host core"
         top_cls = sorted(by_class.items(), key=lambda kv: -kv[1][0])
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,

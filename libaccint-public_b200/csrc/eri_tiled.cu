@@ -131,6 +131,99 @@ __global__ void __launch_bounds__(kWarps * 32) eri_tiled_kernel(QuartetBlock blk
   const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
   const int W = g.LCD + 1;
   const int ncd = g.nc * g.nd, nbcd = g.nb * ncd;
+  // one quartet's geometry, set per quartet below and read by the phases
+  double AB[3], CD[3];
+  // primitive-quartet quantities
+  struct PrimQ {
+    double hz, he, inv, rz, re, T, pref;
+    double PA[3], QC[3], PQ[3];
+  };
+  auto prim_quartet = [&](const double* pb, const double* pk, PrimQ& o) {
+    const double zeta = __ldg(pb + PF_ZETA * sb);
+    o.hz = __ldg(pb + PF_HZ * sb);
+    const double P[3] = {__ldg(pb + PF_PX * sb), __ldg(pb + PF_PY * sb), __ldg(pb + PF_PZ * sb)};
+    o.PA[0] = __ldg(pb + PF_PAX * sb); o.PA[1] = __ldg(pb + PF_PAY * sb); o.PA[2] = __ldg(pb + PF_PAZ * sb);
+    const double cab = __ldg(pb + PF_C * sb);
+    const double eta = __ldg(pk + PF_ZETA * sk);
+    o.he = __ldg(pk + PF_HZ * sk);
+    o.QC[0] = __ldg(pk + PF_PAX * sk); o.QC[1] = __ldg(pk + PF_PAY * sk); o.QC[2] = __ldg(pk + PF_PAZ * sk);
+    o.PQ[0] = P[0] - __ldg(pk + PF_PX * sk);
+    o.PQ[1] = P[1] - __ldg(pk + PF_PY * sk);
+    o.PQ[2] = P[2] - __ldg(pk + PF_PZ * sk);
+    const double ccd = __ldg(pk + PF_C * sk);
+    const double rs = rsqrt(zeta + eta);
+    o.inv = rs * rs;
+    o.rz = eta * o.inv;
+    o.re = zeta * o.inv;
+    o.T = zeta * o.rz * (o.PQ[0] * o.PQ[0] + o.PQ[1] * o.PQ[1] + o.PQ[2] * o.PQ[2]);
+    o.pref = cab * ccd * rs;
+  };
+  // table phase: lane t < 3*nr owns (root r0 + t/3, direction t%3); builds V by the
+  // vertical recurrence, then in place the bra transfer into X and the ket
+  // transfer into H
+  auto table_phase = [&](int r0, int nr, const PrimQ& o) {
+    if (lane >= 3 * nr) return;
+    const int rr = lane / 3, x = lane - 3 * rr;
+    double u, w;
+    rys_root_one<double>(g.n, r0 + rr, o.T, tab, u, w);
+    double* V = Vt + (rr * 3 + x) * g.vsz;
+    const double b00 = 0.5 * o.inv * u, b10 = o.hz - o.hz * o.rz * u, b01 = o.he - o.he * o.re * u;
+    // direction-x components (selects, not runtime-indexed arrays, which would
+    // live in local memory)
+    const double pqx = x == 0 ? o.PQ[0] : x == 1 ? o.PQ[1] : o.PQ[2];
+    const double pax = x == 0 ? o.PA[0] : x == 1 ? o.PA[1] : o.PA[2];
+    const double qcx = x == 0 ? o.QC[0] : x == 1 ? o.QC[1] : o.QC[2];
+    const double pa = pax - o.rz * u * pqx;
+    const double qc = qcx + o.re * u * pqx;
+    V[0] = (x == 2) ? w * o.pref : 1.0;
+    if (g.LAB > 0) V[W] = pa * V[0];
+    for (int e = 1; e < g.LAB; ++e) V[(e + 1) * W] = pa * V[e * W] + e * b10 * V[(e - 1) * W];
+    for (int f = 0; f < g.LCD; ++f)
+      for (int e = 0; e <= g.LAB; ++e) {
+        double v = qc * V[e * W + f];
+        if (f) v += f * b01 * V[e * W + f - 1];
+        if (e) v += e * b00 * V[(e - 1) * W + f];
+        V[e * W + f + 1] = v;
+      }
+    // horizontal transfer, in place: bra levels b = 0..lb of each column f of V
+    // (I(a, b+1) = I(a+1, b) + AB I(a, b)) into X[a][b][f], then ket levels of
+    // each X[a][b][.] into H[a][b][c][d]
+    double* X = Xt + (rr * 3 + x) * g.xsz;
+    double* H = Ht + (rr * 3 + x) * g.hsz;
+    const double ab = x == 0 ? AB[0] : x == 1 ? AB[1] : AB[2];
+    const double cdv = x == 0 ? CD[0] : x == 1 ? CD[1] : CD[2];
+    for (int f = 0; f <= g.LCD; ++f) {
+      for (int a = 0; a < g.EA; ++a) X[(a * g.EB) * W + f] = V[a * W + f];
+      for (int b = 1; b < g.EB; ++b) {
+        for (int a = 0; a + b <= g.LAB; ++a) V[a * W + f] = V[(a + 1) * W + f] + ab * V[a * W + f];
+        for (int a = 0; a < g.EA; ++a) X[(a * g.EB + b) * W + f] = V[a * W + f];
+      }
+    }
+    for (int a = 0; a < g.EA; ++a)
+      for (int b = 0; b < g.EB; ++b) {
+        double* col = X + (a * g.EB + b) * W;
+        double* h = H + (a * g.EB + b) * g.EC * g.ED;
+        for (int c = 0; c < g.EC; ++c) h[c * g.ED] = col[c];
+        for (int d = 1; d < g.ED; ++d) {
+          for (int c = 0; c + d <= g.LCD; ++c) col[c] = col[c + 1] + cdv * col[c];
+          for (int c = 0; c < g.EC; ++c) h[c * g.ED + d] = col[c];
+        }
+      }
+  };
+  // output phase: acc[m] += sum over the batch's roots of Hx Hy Hz at the lane's
+  // output offsets
+  auto output_phase = [&](int nr, const int (&off)[kOut], double (&acc)[kOut]) {
+    for (int rr = 0; rr < nr; ++rr) {
+      const double* Hx = Ht + (rr * 3 + 0) * g.hsz;
+      const double* Hy = Ht + (rr * 3 + 1) * g.hsz;
+      const double* Hz = Ht + (rr * 3 + 2) * g.hsz;
+#pragma unroll
+      for (int m = 0; m < kOut; ++m) {
+        const int o = off[m];
+        if (o >= 0) acc[m] += Hx[o & 1023] * Hy[(o >> 10) & 1023] * Hz[o >> 20];
+      }
+    }
+  };
 
   const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
   const int64_t nw = (int64_t)gridDim.x * kWarps;
@@ -138,6 +231,9 @@ __global__ void __launch_bounds__(kWarps * 32) eri_tiled_kernel(QuartetBlock blk
   const int64_t per = (nq_all + nw - 1) / nw;
   const int64_t tbeg = blk.t_begin + gw * per;
   const int64_t tend = min(blk.total, tbeg + per);
+  // a single primitive quartet per quartet and all roots in one batch: the tables
+  // are built once and serve every output pass
+  const bool single = Kab * Kcd == 1 && g.rb >= g.n && g.npass > 1;
   int p = -1;
   for (int64_t t = tbeg; t < tend; ++t) {
     if (p < 0) {
@@ -147,8 +243,8 @@ __global__ void __launch_bounds__(kWarps * 32) eri_tiled_kernel(QuartetBlock blk
       while (t >= __ldg(blk.offsets + p + 1)) ++p;
     }
     const int q = (blk.qbegin ? __ldg(blk.qbegin + p) : 0) + (int)(t - __ldg(blk.offsets + p));
-    const double AB[3] = {__ldg(blk.bra.AB + p), __ldg(blk.bra.AB + nbra + p), __ldg(blk.bra.AB + 2 * nbra + p)};
-    const double CD[3] = {__ldg(blk.ket.AB + q), __ldg(blk.ket.AB + nket + q), __ldg(blk.ket.AB + 2 * nket + q)};
+    AB[0] = __ldg(blk.bra.AB + p); AB[1] = __ldg(blk.bra.AB + nbra + p); AB[2] = __ldg(blk.bra.AB + 2 * nbra + p);
+    CD[0] = __ldg(blk.ket.AB + q); CD[1] = __ldg(blk.ket.AB + nket + q); CD[2] = __ldg(blk.ket.AB + 2 * nket + q);
     const int fa = __ldg(blk.bra.func_a + p), fb = __ldg(blk.bra.func_b + p);
     const int fc = __ldg(blk.ket.func_a + q), fd = __ldg(blk.ket.func_b + q);
     const double sym = args.mode == MODE_JK ? quartet_weight(blk, p, q) : 0.0;
@@ -171,6 +267,7 @@ __global__ void __launch_bounds__(kWarps * 32) eri_tiled_kernel(QuartetBlock blk
     }
     double smax = 0.0;
     unsigned int nprim_done = 0;
+    bool have_tables = false;
 
     for (int pass = 0; pass < g.npass; ++pass) {
       // packed table offsets of this lane's outputs (x | y << 10 | z << 20), -1 = none
@@ -191,93 +288,42 @@ __global__ void __launch_bounds__(kWarps * 32) eri_tiled_kernel(QuartetBlock blk
         }
       }
 
-      for (int ib = 0; ib < Kab; ++ib) {
-        const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
-        const double qab = __ldg(pb + PF_Q * sb);
-        if (qab * blk.ket.qprim_max < args.prim_eps) break;
-        const double zeta = __ldg(pb + PF_ZETA * sb), hz = __ldg(pb + PF_HZ * sb);
-        const double P[3] = {__ldg(pb + PF_PX * sb), __ldg(pb + PF_PY * sb), __ldg(pb + PF_PZ * sb)};
-        const double PA[3] = {__ldg(pb + PF_PAX * sb), __ldg(pb + PF_PAY * sb), __ldg(pb + PF_PAZ * sb)};
-        const double cab = __ldg(pb + PF_C * sb);
-        for (int ik = 0; ik < Kcd; ++ik) {
-          const double* pk = blk.ket.prim + (size_t)ik * nket + q;
-          const double qcd = __ldg(pk + PF_Q * sk);
-          if (qab * qcd < args.prim_eps) break;
-          if (pass == 0) ++nprim_done;
-          const double eta = __ldg(pk + PF_ZETA * sk), he = __ldg(pk + PF_HZ * sk);
-          const double QC[3] = {__ldg(pk + PF_PAX * sk), __ldg(pk + PF_PAY * sk), __ldg(pk + PF_PAZ * sk)};
-          const double PQ[3] = {P[0] - __ldg(pk + PF_PX * sk), P[1] - __ldg(pk + PF_PY * sk),
-                                P[2] - __ldg(pk + PF_PZ * sk)};
-          const double ccd = __ldg(pk + PF_C * sk);
-          const double rs = rsqrt(zeta + eta);
-          const double inv = rs * rs;
-          const double rz = eta * inv, re = zeta * inv;
-          const double T = zeta * rz * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-          const double pref = cab * ccd * rs;
-          for (int r0 = 0; r0 < g.n; r0 += g.rb) {
-            const int nr = min(g.rb, g.n - r0);
-            // ---- table phase ----
-            if (lane < 3 * nr) {
-              const int rr = lane / 3, x = lane - 3 * rr;
-              double u, w;
-              rys_root_one<double>(g.n, r0 + rr, T, tab, u, w);
-              double* V = Vt + (rr * 3 + x) * g.vsz;
-              const double b00 = 0.5 * inv * u, b10 = hz - hz * rz * u, b01 = he - he * re * u;
-              // direction-x components (selects, not runtime-indexed arrays, which
-              // would live in local memory)
-              const double pqx = x == 0 ? PQ[0] : x == 1 ? PQ[1] : PQ[2];
-              const double pax = x == 0 ? PA[0] : x == 1 ? PA[1] : PA[2];
-              const double qcx = x == 0 ? QC[0] : x == 1 ? QC[1] : QC[2];
-              const double pa = pax - rz * u * pqx;
-              const double qc = qcx + re * u * pqx;
-              V[0] = (x == 2) ? w * pref : 1.0;
-              if (g.LAB > 0) V[W] = pa * V[0];
-              for (int e = 1; e < g.LAB; ++e) V[(e + 1) * W] = pa * V[e * W] + e * b10 * V[(e - 1) * W];
-              for (int f = 0; f < g.LCD; ++f)
-                for (int e = 0; e <= g.LAB; ++e) {
-                  double v = qc * V[e * W + f];
-                  if (f) v += f * b01 * V[e * W + f - 1];
-                  if (e) v += e * b00 * V[(e - 1) * W + f];
-                  V[e * W + f + 1] = v;
-                }
-              // horizontal transfer, in place: bra levels b = 0..lb of each column f
-              // of V (I(a, b+1) = I(a+1, b) + AB I(a, b)) into X[a][b][f], then ket
-              // levels of each X[a][b][.] into H[a][b][c][d]
-              double* X = Xt + (rr * 3 + x) * g.xsz;
-              double* H = Ht + (rr * 3 + x) * g.hsz;
-              const double ab = x == 0 ? AB[0] : x == 1 ? AB[1] : AB[2];
-              const double cdv = x == 0 ? CD[0] : x == 1 ? CD[1] : CD[2];
-              for (int f = 0; f <= g.LCD; ++f) {
-                for (int a = 0; a < g.EA; ++a) X[(a * g.EB) * W + f] = V[a * W + f];
-                for (int b = 1; b < g.EB; ++b) {
-                  for (int a = 0; a + b <= g.LAB; ++a) V[a * W + f] = V[(a + 1) * W + f] + ab * V[a * W + f];
-                  for (int a = 0; a < g.EA; ++a) X[(a * g.EB + b) * W + f] = V[a * W + f];
-                }
-              }
-              for (int a = 0; a < g.EA; ++a)
-                for (int b = 0; b < g.EB; ++b) {
-                  double* col = X + (a * g.EB + b) * W;
-                  double* h = H + (a * g.EB + b) * g.EC * g.ED;
-                  for (int c = 0; c < g.EC; ++c) h[c * g.ED] = col[c];
-                  for (int d = 1; d < g.ED; ++d) {
-                    for (int c = 0; c + d <= g.LCD; ++c) col[c] = col[c + 1] + cdv * col[c];
-                    for (int c = 0; c < g.EC; ++c) h[c * g.ED + d] = col[c];
-                  }
-                }
+      if (single) {
+        // one primitive quartet and one root batch: its tables, built in the first
+        // pass, stay in shared memory for the later passes
+        if (pass == 0) {
+          const double* pb = blk.bra.prim + p;
+          const double* pk = blk.ket.prim + q;
+          const double qab = __ldg(pb + PF_Q * sb), qcd = __ldg(pk + PF_Q * sk);
+          have_tables = !(qab * qcd < args.prim_eps);
+          if (have_tables) {
+            ++nprim_done;
+            PrimQ pq;
+            prim_quartet(pb, pk, pq);
+            table_phase(0, g.n, pq);
+          }
+          __syncwarp();
+        }
+        if (have_tables) output_phase(g.n, off, acc);
+      } else {
+        for (int ib = 0; ib < Kab; ++ib) {
+          const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
+          const double qab = __ldg(pb + PF_Q * sb);
+          if (qab * blk.ket.qprim_max < args.prim_eps) break;
+          for (int ik = 0; ik < Kcd; ++ik) {
+            const double* pk = blk.ket.prim + (size_t)ik * nket + q;
+            const double qcd = __ldg(pk + PF_Q * sk);
+            if (qab * qcd < args.prim_eps) break;
+            if (pass == 0) ++nprim_done;
+            PrimQ pq;
+            prim_quartet(pb, pk, pq);
+            for (int r0 = 0; r0 < g.n; r0 += g.rb) {
+              const int nr = min(g.rb, g.n - r0);
+              table_phase(r0, nr, pq);
+              __syncwarp();
+              output_phase(nr, off, acc);
+              __syncwarp();
             }
-            __syncwarp();
-            // ---- output phase ----
-            for (int rr = 0; rr < nr; ++rr) {
-              const double* Hx = Ht + (rr * 3 + 0) * g.hsz;
-              const double* Hy = Ht + (rr * 3 + 1) * g.hsz;
-              const double* Hz = Ht + (rr * 3 + 2) * g.hsz;
-#pragma unroll
-              for (int m = 0; m < kOut; ++m) {
-                const int o = off[m];
-                if (o >= 0) acc[m] += Hx[o & 1023] * Hy[(o >> 10) & 1023] * Hz[o >> 20];
-              }
-            }
-            __syncwarp();
           }
         }
       }

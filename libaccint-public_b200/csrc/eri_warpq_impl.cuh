@@ -14,7 +14,10 @@
 //      and adds sum_r Ix Iy Iz to them in registers.
 // After the last primitive quartet, once per contracted quartet: G goes to shared
 // memory, the horizontal transfer in closed form (binomial sums, the same transfer
-// as eri_device.cuh) gives first (ab|f0] and then (ab|cd), which is normalized and
+// as eri_device.cuh; the terms of every component, their integer coefficients and
+// target indices are tabulated per class in shared memory when the block starts,
+// and the quartet's AB/CD powers once per quartet) gives first (ab|f0] and then
+// (ab|cd), which is normalized and
 // digested by the lanes into the six Fock blocks (lane-owned sums, no shared-memory
 // atomics).  J'_ab accumulates in shared memory while consecutive quartets of the
 // warp keep their bra pair and goes to global memory once per bra pair; the other
@@ -39,6 +42,16 @@ constexpr int kWarpqMaxG = 1152;    // (e0|f0) integrals per quartet: 36 per lan
 constexpr int kWarpqWarps = 4;      // warps per block
 
 __host__ __device__ constexpr int warpq_max(int a, int b) { return a > b ? a : b; }
+// most terms prod_x (b_x + 1) of a component of shell l
+__host__ __device__ constexpr int warpq_max_terms(int l) {
+  int m = 1;
+  for (int x = l; x >= 0; --x)
+    for (int y = l - x; y >= 0; --y) {
+      const int t = (x + 1) * (y + 1) * (l - x - y + 1);
+      m = t > m ? t : m;
+    }
+  return m;
+}
 
 template <int LA, int LB, int LC, int LD>
 struct WarpqClass {
@@ -57,7 +70,10 @@ struct WarpqClass {
   static constexpr int S_BUF = warpq_max(NG, warpq_max(NX, NO));
   static constexpr int OFF_B0 = S_V, OFF_B1 = OFF_B0 + S_BUF, OFF_D = OFF_B1 + S_BUF;
   static constexpr int OFF_JAB = OFF_D + NACC;
-  static constexpr int PER_WARP = ((OFF_JAB + NAB) + 1) & ~1;
+  // transfer terms: a shell-b component takes prod_x (b_x + 1) terms k <= b
+  static constexpr int MTB = warpq_max_terms(LB), MTD = warpq_max_terms(LD);
+  static constexpr int OFF_CB = OFF_JAB + NAB, OFF_CD = OFF_CB + NB * MTB;
+  static constexpr int PER_WARP = ((OFF_CD + ND * MTD) + 1) & ~1;
   // blocks per SM the register allocation targets: the warp's latency (dependent
   // global loads, warp syncs) is hidden by other warps, so the small classes are
   // held to few registers (estimate: G, its offsets, one lane's 2D table, ~40 more)
@@ -104,10 +120,51 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
       s_norm[sh][k] = norm_factor(l, k);
     }
   }
+  // transfer tables of the class: for bra component b, term t < s_bn[b] is the
+  // shift k <= b with integer coefficient prod_x C(b_x, k_x) (s_bc) and powers
+  // b - k of AB (s_bp, 4 bits each); s_be[a][b][t] is the (e0| index of a + k.
+  // The same for the ket (d, c, CD).
+  constexpr int MTB = C::MTB, MTD = C::MTD;
+  __shared__ int s_bn[NB], s_bc[NB * MTB], s_bp[NB * MTB], s_be[NAB * MTB];
+  __shared__ int s_dn[ND], s_dc[ND * MTD], s_dp[ND * MTD], s_df[NC * ND * MTD];
+  for (int i = threadIdx.x; i < NAB + NC * ND; i += blockDim.x) {
+    const bool bra = i < NAB;
+    const int u = bra ? i / NB : (i - NAB) / ND;      // a (or c)
+    const int v = bra ? i % NB : (i - NAB) % ND;      // b (or d)
+    const int lu = bra ? LA : LC, lv = bra ? LB : LD;
+    const int cu = cart_comp(lu, u), cv = cart_comp(lv, v);
+    const int vx = comp_x(cv), vy = comp_y(cv), vz = comp_z(cv);
+    int t = 0;
+    for (int kx = 0; kx <= vx; ++kx)
+      for (int ky = 0; ky <= vy; ++ky)
+        for (int kz = 0; kz <= vz; ++kz, ++t) {
+          const int l = lu + kx + ky + kz;
+          const int e = ncart_before(lu, l) + cart_index(comp_x(cu) + kx, comp_y(cu) + ky, comp_z(cu) + kz);
+          if (bra) {
+            s_be[i * MTB + t] = e;
+            if (u == 0) {
+              s_bc[v * MTB + t] = warpq_binom(vx, kx) * warpq_binom(vy, ky) * warpq_binom(vz, kz);
+              s_bp[v * MTB + t] = (vx - kx) | ((vy - ky) << 4) | ((vz - kz) << 8);
+            }
+          } else {
+            s_df[(i - NAB) * MTD + t] = e;
+            if (u == 0) {
+              s_dc[v * MTD + t] = warpq_binom(vx, kx) * warpq_binom(vy, ky) * warpq_binom(vz, kz);
+              s_dp[v * MTD + t] = (vx - kx) | ((vy - ky) << 4) | ((vz - kz) << 8);
+            }
+          }
+        }
+    if (u == 0) {
+      if (bra) s_bn[v] = t;
+      else s_dn[v] = t;
+    }
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   double* const Vs = smem_q + (size_t)warp * C::PER_WARP;
+  double* const CoB = Vs + C::OFF_CB;   // per quartet: coefficient of bra term (b, t)
+  double* const CoD = Vs + C::OFF_CD;   // per quartet: coefficient of ket term (d, t)
   double* const B0 = Vs + C::OFF_B0;
   double* const B1 = Vs + C::OFF_B1;
   double* const Ds = Vs + C::OFF_D;
@@ -277,49 +334,44 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
     const double CDx = __ldg(blk.ket.AB + q), CDy = __ldg(blk.ket.AB + nket + q),
                  CDz = __ldg(blk.ket.AB + 2 * nket + q);
     __syncwarp();
+    // this quartet's transfer coefficients C(b, k) AB^(b-k) and C(d, k) CD^(d-k)
+    for (int i = lane; i < NB * MTB + ND * MTD; i += 32) {
+      const bool bra = i < NB * MTB;
+      const int k = bra ? i : i - NB * MTB;
+      const int pk = bra ? s_bp[k] : s_dp[k];
+      const double cx = bra ? ABx : CDx, cy = bra ? ABy : CDy, cz = bra ? ABz : CDz;
+      double v = bra ? (double)s_bc[k] : (double)s_dc[k];
+      v *= warpq_pow(cx, pk & 15) * warpq_pow(cy, (pk >> 4) & 15) * warpq_pow(cz, pk >> 8);
+      (bra ? CoB : CoD)[k] = v;
+    }
+    __syncwarp();
     // bra transfer: (ab|f0] = sum_k prod_x C(b_x, k_x) AB_x^(b_x - k_x) (a+k 0|f0]
     for (int j = lane; j < C::NX; j += 32) {
       const int ab = j / NF, f = j - ab * NF;
-      const int a = ab / NB, b = ab - a * NB;
-      const int ca = s_comp[0][a], cb = s_comp[1][b];
-      const int ax = comp_x(ca), ay = comp_y(ca), az = comp_z(ca);
-      const int bx = comp_x(cb), by = comp_y(cb), bz = comp_z(cb);
+      const int b = ab % NB;
+      const int nt = s_bn[b];
+      const int* ei = s_be + ab * MTB;
+      const double* co = CoB + b * MTB;
       double s = 0.0;
-      for (int kx = 0; kx <= bx; ++kx) {
-        const double cx = warpq_binom(bx, kx) * warpq_pow(ABx, bx - kx);
-        for (int ky = 0; ky <= by; ++ky) {
-          const double cy = cx * warpq_binom(by, ky) * warpq_pow(ABy, by - ky);
-          for (int kz = 0; kz <= bz; ++kz) {
-            const int l = LA + kx + ky + kz;
-            const int e = ncart_before(LA, l) + cart_index(ax + kx, ay + ky, az + kz);
-            s += cy * warpq_binom(bz, kz) * warpq_pow(ABz, bz - kz) * B0[e * NF + f];
-          }
-        }
-      }
+#pragma unroll
+      for (int t = 0; t < MTB; ++t)
+        if (t < nt) s += co[t] * B0[ei[t] * NF + f];
       B1[j] = s;
     }
     __syncwarp();
     // ket transfer and normalization: (ab|cd) into B0[ab][c][d]
     for (int j = lane; j < C::NO; j += 32) {
       const int ab = j / NCD, cd = j - ab * NCD;
-      const int c = cd / ND, d = cd - c * ND;
-      const int a = ab / NB, b = ab - a * NB;
-      const int cc = s_comp[2][c], cdc = s_comp[3][d];
-      const int cx0 = comp_x(cc), cy0 = comp_y(cc), cz0 = comp_z(cc);
-      const int dx = comp_x(cdc), dy = comp_y(cdc), dz = comp_z(cdc);
+      const int d = cd % ND;
+      const int nt = s_dn[d];
+      const int* fi = s_df + cd * MTD;
+      const double* co = CoD + d * MTD;
       const double* row = B1 + ab * NF;
       double s = 0.0;
-      for (int kx = 0; kx <= dx; ++kx) {
-        const double wx = warpq_binom(dx, kx) * warpq_pow(CDx, dx - kx);
-        for (int ky = 0; ky <= dy; ++ky) {
-          const double wy = wx * warpq_binom(dy, ky) * warpq_pow(CDy, dy - ky);
-          for (int kz = 0; kz <= dz; ++kz) {
-            const int l = LC + kx + ky + kz;
-            const int f = ncart_before(LC, l) + cart_index(cx0 + kx, cy0 + ky, cz0 + kz);
-            s += wy * warpq_binom(dz, kz) * warpq_pow(CDz, dz - kz) * row[f];
-          }
-        }
-      }
+#pragma unroll
+      for (int t = 0; t < MTD; ++t)
+        if (t < nt) s += co[t] * row[fi[t]];
+      const int a = ab / NB, b = ab - a * NB, c = cd / ND;
       B0[j] = s * s_norm[0][a] * s_norm[1][b] * s_norm[2][c] * s_norm[3][d];
     }
     __syncwarp();
