@@ -155,6 +155,17 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
           }
         }
     if (u == 0) {
+      // unused terms: coefficient 0, no powers (every entry of the tables is read
+      // when a quartet's coefficients are formed)
+      for (int r = t; r < (bra ? MTB : MTD); ++r) {
+        if (bra) {
+          s_bc[v * MTB + r] = 0;
+          s_bp[v * MTB + r] = 0;
+        } else {
+          s_dc[v * MTD + r] = 0;
+          s_dp[v * MTD + r] = 0;
+        }
+      }
       if (bra) s_bn[v] = t;
       else s_dn[v] = t;
     }
@@ -341,7 +352,7 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
       const int pk = bra ? s_bp[k] : s_dp[k];
       const double cx = bra ? ABx : CDx, cy = bra ? ABy : CDy, cz = bra ? ABz : CDz;
       double v = bra ? (double)s_bc[k] : (double)s_dc[k];
-      v *= warpq_pow(cx, pk & 15) * warpq_pow(cy, (pk >> 4) & 15) * warpq_pow(cz, pk >> 8);
+      v *= warpq_pow(cx, pk & 15) * warpq_pow(cy, (pk >> 4) & 15) * warpq_pow(cz, (pk >> 8) & 15);
       (bra ? CoB : CoD)[k] = v;
     }
     __syncwarp();
