@@ -10,6 +10,12 @@
  *   lai::GpuFockBuilder ~ consumers::GpuFockBuilder: device J/K, D uploaded by
  *                       set_density, results copied back by get_*
  *                       (include/libaccint/consumers/fock_builder_gpu.hpp:46-159)
+ *   lai::Operator / PointChargeParams and Engine::compute_1e, compute_overlap_matrix,
+ *                       compute_kinetic_matrix, compute_nuclear_matrix
+ *                       (include/libaccint/engine/engine.hpp:166-201, 831-900;
+ *                       include/libaccint/operators/operator_types.hpp:50-60)
+ *   lai::BasisSet::from_bse_json ~ data::BseJsonParser::parse
+ *                       (src/shared/data/bse_json_parser.cpp:27-140)
  *
  * Errors become exceptions here (std::invalid_argument for LAI_EINVAL,
  * std::runtime_error otherwise), as in the reference; the C ABI itself never
@@ -62,6 +68,16 @@ class BasisSet {
                            atom.data(), 0, &h_),
           "BasisSet");
   }
+  // Basis Set Exchange JSON text on atoms (atomic numbers Z, positions xyz[3*i], Bohr).
+  static BasisSet from_bse_json(const std::string& json, const std::vector<int>& Z,
+                                const std::vector<double>& xyz) {
+    if (xyz.size() != 3 * Z.size()) throw std::invalid_argument("BasisSet::from_bse_json: xyz size");
+    lai_basis* h = nullptr;
+    check(lai_basis_from_bse_json(json.data(), json.size(), (int)Z.size(), Z.data(), xyz.data(), &h),
+          "BasisSet::from_bse_json");
+    return BasisSet(h);
+  }
+  BasisSet(BasisSet&& o) noexcept : h_(o.h_) { o.h_ = nullptr; }
   ~BasisSet() { lai_basis_destroy(h_); }
   BasisSet(const BasisSet&) = delete;
   BasisSet& operator=(const BasisSet&) = delete;
@@ -69,11 +85,24 @@ class BasisSet {
   const lai_basis* handle() const { return h_; }
 
  private:
+  explicit BasisSet(lai_basis* h) : h_(h) {}
   lai_basis* h_ = nullptr;
 };
 
+// Structure-of-arrays point charges (nuclei: charge = atomic number).
+struct PointChargeParams {
+  std::vector<double> x, y, z, charge;
+  std::size_t n_centers() const { return charge.size(); }
+};
+
 struct Operator {
+  enum class Kind { Coulomb, Overlap, Kinetic, Nuclear };
+  Kind kind = Kind::Coulomb;
+  PointChargeParams charges;
   static Operator coulomb() { return Operator{}; }
+  static Operator overlap() { return Operator{Kind::Overlap, {}}; }
+  static Operator kinetic() { return Operator{Kind::Kinetic, {}}; }
+  static Operator nuclear(const PointChargeParams& c) { return Operator{Kind::Nuclear, c}; }
 };
 
 class FockBuilder {
@@ -171,7 +200,8 @@ class Engine {
   Engine& operator=(const Engine&) = delete;
 
   // Engine::compute(Operator::coulomb(), FockBuilder&): J/K added to the builder's.
-  void compute(const Operator&, FockBuilder& fb) {
+  void compute(const Operator& op, FockBuilder& fb) {
+    if (op.kind != Operator::Kind::Coulomb) throw std::invalid_argument("Engine::compute: not a two-electron operator");
     if (!fb.density()) throw std::logic_error("FockBuilder: density matrix not set");
     if (fb.nbf() != nbf_) throw std::invalid_argument("Engine::compute: nbf mismatch");
     std::vector<double> J(nbf_ * nbf_), K(nbf_ * nbf_);
@@ -180,10 +210,43 @@ class Engine {
   }
   // Engine::compute(Operator::coulomb(), GpuFockBuilder&): device J/K on the
   // builder's stream (overwritten, as after reset()).
-  void compute(const Operator&, GpuFockBuilder& fb) {
+  void compute(const Operator& op, GpuFockBuilder& fb) {
+    if (op.kind != Operator::Kind::Coulomb) throw std::invalid_argument("Engine::compute: not a two-electron operator");
     if (fb.nbf() != nbf_) throw std::invalid_argument("Engine::compute: nbf mismatch");
     check(lai_jk_build_device(h_, fb.d_D(), fb.d_J(), fb.d_K(), fb.stream(), nullptr, nullptr),
           "Engine::compute");
+  }
+  // One-electron matrices (nbf x nbf, row-major) of Operator::overlap(), kinetic()
+  // or nuclear(charges); Engine::compute_1e(op, result) of the reference.
+  void compute_1e(const Operator& op, std::vector<double>& result) {
+    result.assign(nbf_ * nbf_, 0.0);
+    int code = LAI_OP_OVERLAP;
+    std::vector<double> xyz, q;
+    switch (op.kind) {
+      case Operator::Kind::Overlap: code = LAI_OP_OVERLAP; break;
+      case Operator::Kind::Kinetic: code = LAI_OP_KINETIC; break;
+      case Operator::Kind::Nuclear: {
+        code = LAI_OP_NUCLEAR;
+        const auto& c = op.charges;
+        const std::size_t n = c.n_centers();
+        if (c.x.size() != n || c.y.size() != n || c.z.size() != n)
+          throw std::invalid_argument("compute_1e: PointChargeParams sizes differ");
+        for (std::size_t i = 0; i < n; ++i) {
+          xyz.insert(xyz.end(), {c.x[i], c.y[i], c.z[i]});
+          q.push_back(c.charge[i]);
+        }
+        break;
+      }
+      default: throw std::invalid_argument("compute_1e: not a one-electron operator");
+    }
+    check(lai_one_electron(h_, code, (int)q.size(), xyz.empty() ? nullptr : xyz.data(),
+                           q.empty() ? nullptr : q.data(), result.data()),
+          "Engine::compute_1e");
+  }
+  void compute_overlap_matrix(std::vector<double>& result) { compute_1e(Operator::overlap(), result); }
+  void compute_kinetic_matrix(std::vector<double>& result) { compute_1e(Operator::kinetic(), result); }
+  void compute_nuclear_matrix(const PointChargeParams& charges, std::vector<double>& result) {
+    compute_1e(Operator::nuclear(charges), result);
   }
   lai_engine* handle() const { return h_; }
 

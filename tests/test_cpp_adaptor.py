@@ -27,6 +27,17 @@ def test_adaptor_compiles_and_links(tmp_path):
     assert _build(tmp_path).exists()
 
 
+def test_one_electron_adaptor_compiles_and_links(tmp_path):
+    exe = tmp_path / "one_electron_adaptor"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+           os.path.join(ROOT, "tests", "cpp", "one_electron_adaptor.cpp"), "-o", str(exe), "-L", LIBDIR,
+           "-laccint_b200", "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath," + LIBDIR,
+           "-Wl,-rpath,/usr/local/cuda/lib64"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert exe.exists()
+
+
 @pytest.mark.gpu
 def test_adaptor_jk_matches_engine(tmp_path, lai):
     exe = _build(tmp_path)
