@@ -564,9 +564,16 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
   const int64_t cap = (int64_t)num_sms * per_sm;
   const int grid = (int)(want < cap ? want : cap);
   // chunks per super-chunk (consecutive chunks a warp takes, one bra search per
-  // super-chunk): the autotuner chose 1 for most launches of the benchmark
-  // systems (longer runs load-balance worse), so 1 is the default
-  const int ksuper = tune.ksuper > 0 ? tune.ksuper : 1;
+  // super-chunk; the warp stays on neighbouring bra pairs and ket rows).  On the
+  // large launches of (H2O)64/cc-pVDZ the autotuner chose 16 where a quartet has
+  // at most 9 primitive quartets and 4 above; a launch keeps at least 8
+  // super-chunks per warp for load balance, so small launches stay at 1.
+  int ksuper = tune.ksuper;
+  if (ksuper <= 0) {
+    const int64_t warps = (int64_t)grid * (threads / 32);
+    const int64_t kmax = (int64_t)Kab * blk.ket.Ka * blk.ket.Kb <= 9 ? 16 : 4;
+    ksuper = (int)std::max<int64_t>(1, std::min<int64_t>(kmax, nchunks / (warps * 8)));
+  }
   kern<<<grid, threads, smem, stream>>>(blk, args, tab, ksuper, ps);
   return cudaGetLastError() == cudaSuccess ? 1 : -3;
 }
