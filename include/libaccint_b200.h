@@ -101,6 +101,9 @@ typedef struct {
                                (default), 0 = keep every primitive quartet       */
 } lai_engine_opts;
 LAI_API void lai_engine_opts_default(lai_engine_opts* opts);
+/* All engines of one process use one device: creating an engine on another
+ * device than the process's first engine returns LAI_ENOTSUP (run one process
+ * per GPU, as the multi-GPU build does). */
 LAI_API int lai_engine_create(const lai_basis* basis, const lai_engine_opts* opts, lai_engine** out);
 LAI_API void lai_engine_destroy(lai_engine* engine);
 /* Schwarz bounds Q[i*nshell+j] = sqrt(max |(ij|ij)|) of all shell pairs

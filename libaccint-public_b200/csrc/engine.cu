@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <chrono>
 #include <cmath>
@@ -830,6 +831,14 @@ int create_engine(const lai_basis* basis, std::unique_ptr<lai_basis> merged, con
   int ndev = 0;
   LAI_CUDA_TRY(cudaGetDeviceCount(&ndev));
   if (o.device < 0 || o.device >= ndev) return fail(LAI_EINVAL, "lai_engine_create: bad device");
+  // The kernel launchers set their launch attributes (dynamic shared-memory
+  // limits) and cache occupancies once per process, and CUDA keeps those per
+  // device: every engine of a process therefore uses the first engine's device.
+  static std::atomic<int> process_device{-1};
+  int first = -1;
+  if (!process_device.compare_exchange_strong(first, o.device) && first != o.device)
+    return fail(LAI_ENOTSUP, "lai_engine_create: this process already runs engines on another CUDA device "
+                             "(one device per process: run one process per GPU)");
   LAI_CUDA_TRY(cudaSetDevice(o.device));
   auto E = std::make_unique<lai_engine>();
   if (merged) {
