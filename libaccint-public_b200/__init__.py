@@ -5,6 +5,6 @@ directory name is not a Python identifier).
 """
 from ._lib import LibAccIntError, lib  # noqa: F401
 from .basis import Atom, BasisSet, Shell, basis_data, cart_to_sph_matrix, point_charges  # noqa: F401
-from .engine import (BatchedEngine, Engine, FockBuilder, Operator, ScreeningOptions, jk,  # noqa: F401
+from .engine import (BatchedEngine, Engine, FockBuilder, GpuFockBuilder, Operator, ScreeningOptions, jk,  # noqa: F401
                      probe_fp64_peak)
 from . import autograd, df, molecules, scf, workloads  # noqa: F401

@@ -87,6 +87,61 @@ class FockBuilder:
         self.K[:] = 0.0
 
 
+class GpuFockBuilder:
+    """Device J/K accumulator (reference consumers::GpuFockBuilder,
+    include/libaccint/consumers/fock_builder_gpu.hpp:46-159, and its Python binding,
+    python/src/advanced_bindings.cpp:680-749).  D, J and K are float64 torch
+    tensors on the device (``d_D``, ``d_J``, ``d_K``); set_density uploads D,
+    get_coulomb_matrix / get_exchange_matrix / get_fock_matrix download.  J and K
+    accumulate across Engine.compute calls until reset().  As in the reference
+    binding, ``nbf()`` is a method and get_fock_matrix defaults to
+    exchange_fraction = 1.0."""
+
+    def __init__(self, nbf, device=0):
+        import torch
+        self._torch = torch
+        self._nbf = int(nbf)
+        self.device = torch.device("cuda", device)
+        self.d_D = torch.zeros((self._nbf, self._nbf), dtype=torch.float64, device=self.device)
+        self.d_J = torch.zeros_like(self.d_D)
+        self.d_K = torch.zeros_like(self.d_D)
+        self.has_density = False
+        self.last_report = None
+
+    def nbf(self):
+        return self._nbf
+
+    def set_density(self, D):
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        if D.size != self._nbf * self._nbf:
+            raise ValueError("Density matrix must have nbf*nbf elements")
+        self.d_D.copy_(self._torch.from_numpy(D.reshape(self._nbf, self._nbf)))
+        self.has_density = True
+
+    def get_coulomb_matrix(self):
+        return self.d_J.cpu().numpy()
+
+    def get_exchange_matrix(self):
+        return self.d_K.cpu().numpy()
+
+    def get_fock_matrix(self, H_core, exchange_fraction=1.0):
+        H = np.asarray(H_core, dtype=np.float64)
+        if H.size != self._nbf * self._nbf:
+            raise ValueError("H_core must have nbf*nbf elements")
+        Hd = self._torch.from_numpy(np.ascontiguousarray(H).reshape(self._nbf, self._nbf)).to(self.device)
+        return (Hd + self.d_J - exchange_fraction * self.d_K).cpu().numpy()
+
+    def reset(self):
+        self.d_J.zero_()
+        self.d_K.zero_()
+
+    def synchronize(self):
+        self._torch.cuda.synchronize(self.device)
+
+    def __repr__(self):
+        return f"GpuFockBuilder(nbf={self._nbf})"
+
+
 class Engine:
     def __init__(self, basis, threshold=1e-12, device=0, prim_threshold=None):
         """``prim_threshold``: primitive-quartet cut (None = 1e-3 * threshold, 0 = off)."""
@@ -319,6 +374,8 @@ class Engine:
     def compute_and_consume(self, op, consumer, screening=None):
         if not op.is_two_electron():
             raise ValueError("compute_and_consume requires a two-electron operator")
+        if isinstance(consumer, GpuFockBuilder):
+            return self._consume_device(consumer, screening)
         if consumer.D is None:
             raise RuntimeError("FockBuilder::accumulate called without density matrix")
         if consumer.nbf != self.basis.nbf:
@@ -333,6 +390,26 @@ class Engine:
 
     def compute(self, op, consumer):
         self.compute_and_consume(op, consumer)
+
+    def _consume_device(self, fb, screening):
+        # device J/K of fb.d_D on torch's current stream of fb's device, added to
+        # fb.d_J / fb.d_K (the builder accumulates until reset())
+        torch = fb._torch
+        if not fb.has_density:
+            raise RuntimeError("GpuFockBuilder: density matrix not set")
+        if fb.nbf() != self.basis.nbf:
+            raise ValueError("GpuFockBuilder nbf does not match the basis")
+        if fb.device.index != self.device:
+            raise ValueError(f"GpuFockBuilder is on cuda:{fb.device.index}, the engine on cuda:{self.device}")
+        if screening is not None and screening.enabled and screening.threshold != self.threshold:
+            raise ValueError("screening threshold differs from the engine's; build an Engine "
+                             "with threshold=%g" % screening.threshold)
+        J = torch.empty_like(fb.d_J)
+        K = torch.empty_like(fb.d_K)
+        stream = torch.cuda.current_stream(fb.device)
+        fb.last_report = self.jk_device(fb.d_D.data_ptr(), J.data_ptr(), K.data_ptr(), stream=stream.cuda_stream)
+        fb.d_J.add_(J)
+        fb.d_K.add_(K)
 
     def close(self):
         if getattr(self, "_h", None) is not None:
