@@ -6,6 +6,9 @@
 * ``reference()``   -- _ref/libref_oracle.so, the UNMODIFIED reference CPU code
   compiled from its own sources by oracle/Makefile, behind ref_shim.cpp.  None when
   it was not built (the reference tree is absent).
+* ``reference_gpu()`` -- _ref/libref_gpu.so, the reference's own GPU route (its CUDA
+  sources for sm_100a behind ref_gpu_shim.cu, ``make -C oracle refgpu``), used only to
+  time the reference kernel on the same device (ref_gpu_bench.py).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
 use this module.  The product (libaccint-public_b200) never imports it.
@@ -19,6 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT = os.path.join(HERE, "liboracle.so")
 REFERENCE = os.path.join(HERE, "_ref", "libref_oracle.so")
+REFERENCE_GPU = os.path.join(HERE, "_ref", "libref_gpu.so")
 
 _P, _I, _D, _L = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
 _orc = None
@@ -101,6 +105,75 @@ def reference():
         L.ref_df_jk.argtypes = [_P, _P, _P, _P, _P]
         _ref = L
     return _ref
+
+
+_ref_gpu = None
+
+
+def reference_gpu():
+    """The reference's own GPU route (make -C oracle refgpu), or None if not built."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not os.path.exists(REFERENCE_GPU):
+            return None
+        L = ctypes.CDLL(REFERENCE_GPU)
+        L.refgpu_last_error.restype = ctypes.c_char_p
+        L.refgpu_basis_create.restype = _P
+        L.refgpu_basis_create.argtypes = [_I, _P, _P, _P, _P, _P]
+        L.refgpu_basis_free.argtypes = [_P]
+        for f in ("refgpu_nbf", "refgpu_nsets"):
+            getattr(L, f).restype = _L
+            getattr(L, f).argtypes = [_P]
+        L.refgpu_unit_size.argtypes = [_P, _L, _P, _P]
+        L.refgpu_jk.argtypes = [_P, _P, _P, _P, _L, _L, _P, _P]
+        _ref_gpu = L
+    return _ref_gpu
+
+
+class RefGpuBasis:
+    """A basis inside the reference's GPU route (raw coefficients; the reference
+    Shell constructor normalizes them).  Units are the ordered ShellSet 4-tuples."""
+
+    def __init__(self, basis):
+        L = reference_gpu()
+        if L is None:
+            raise RuntimeError("oracle/_ref/libref_gpu.so not built (make -C oracle refgpu)")
+        self._L = L
+        l, nprim, centers, exps, coefs, _ = basis.arrays()
+        self._keep = [np.ascontiguousarray(a, dtype=t) for a, t in
+                      ((l, np.int32), (nprim, np.int32), (centers, np.float64), (exps, np.float64),
+                       (coefs, np.float64))]
+        a = self._keep
+        self._h = L.refgpu_basis_create(len(a[0]), *(x.ctypes.data for x in a))
+        if not self._h:
+            raise RuntimeError(L.refgpu_last_error().decode())
+        self.nbf = int(L.refgpu_nbf(self._h))
+        self.nsets = int(L.refgpu_nsets(self._h))
+        self.nunits = self.nsets ** 4
+
+    def unit_size(self, u):
+        """(shell quartets, integral doubles) of unit u."""
+        q, v = ctypes.c_long(), ctypes.c_long()
+        if self._L.refgpu_unit_size(self._h, u, ctypes.byref(q), ctypes.byref(v)) != 0:
+            raise ValueError("bad unit")
+        return q.value, v.value
+
+    def jk(self, D, u_begin=0, u_end=None):
+        """(J, K, device ms, shell quartets) of units [u_begin, u_end) (all = full J/K)."""
+        u_end = self.nunits if u_end is None else u_end
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        J = np.zeros((self.nbf, self.nbf))
+        K = np.zeros((self.nbf, self.nbf))
+        ms, nq = ctypes.c_double(), ctypes.c_long()
+        if self._L.refgpu_jk(self._h, D.ctypes.data, J.ctypes.data, K.ctypes.data, u_begin, u_end,
+                             ctypes.byref(ms), ctypes.byref(nq)) != 0:
+            raise RuntimeError(self._L.refgpu_last_error().decode())
+        return J, K, ms.value, nq.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._L.refgpu_basis_free(self._h)
+            self._h = None
 
 
 def ref_cart_to_sph(l):
