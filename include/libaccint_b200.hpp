@@ -45,6 +45,9 @@
 
 #include "libaccint_b200.h"
 
+#define LAI_STR_(x) #x
+#define LAI_STR(x) LAI_STR_(x)
+
 namespace lai {
 
 inline void check(int rc, const char* what) {
@@ -54,11 +57,28 @@ inline void check(int rc, const char* what) {
   throw std::runtime_error(msg);
 }
 
+// The reference's scalar and size types (include/libaccint/core/types.hpp).
+using Real = double;
+using Size = std::size_t;
+
+struct Point3D {
+  double x = 0.0, y = 0.0, z = 0.0;
+};
+
+// Library identity: this build has one backend, the B200 one.
+inline const char* version() { return "libaccint-b200 (C ABI " LAI_STR(LAI_ABI_VERSION) ")"; }
+inline bool has_cuda_backend() { return true; }
+
 struct Shell {
-  int l;
-  double center[3];
+  int l = 0;
+  double center[3] = {0.0, 0.0, 0.0};
   std::vector<double> exps, coefs;  // raw contraction coefficients
   int atom = -1;
+  Shell() = default;
+  // Shell(am, center, exps, coefs) (src/shared/basis/shell.cpp:163-187); the
+  // library normalizes the raw coefficients when the BasisSet is built.
+  Shell(int am, Point3D c, std::vector<double> e, std::vector<double> k)
+      : l(am), center{c.x, c.y, c.z}, exps(std::move(e)), coefs(std::move(k)) {}
 };
 
 // Shells of one angular momentum and primitive count, by their index in the
@@ -415,6 +435,18 @@ class Engine {
   Engine(const Engine&) = delete;
   Engine& operator=(const Engine&) = delete;
 
+  // The reference's backend hint (include/libaccint/engine/dispatch_policy.hpp:41-47):
+  // every hint that allows the GPU runs the B200 path; ForceCPU throws
+  // std::invalid_argument, since this build has no CPU path.
+  enum class BackendHint { Auto, ForceCPU, ForceGPU, PreferCPU, PreferGPU };
+  template <class Builder>
+  void compute(const Operator& op, Builder& fb, BackendHint hint) {
+    if (hint == BackendHint::ForceCPU)
+      throw std::invalid_argument("Engine::compute: BackendHint::ForceCPU -- this build has no CPU backend");
+    compute(op, fb);
+  }
+  bool gpu_available() const { return true; }  // an Engine exists only on a usable device
+
   // Engine::compute(Operator::coulomb(), FockBuilder&): J/K added to the builder's.
   void compute(const Operator& op, FockBuilder& fb) {
     if (op.kind != Operator::Kind::Coulomb) throw std::invalid_argument("Engine::compute: not a two-electron operator");
@@ -463,6 +495,18 @@ class Engine {
   void compute_kinetic_matrix(std::vector<double>& result) { compute_1e(Operator::kinetic(), result); }
   void compute_nuclear_matrix(const PointChargeParams& charges, std::vector<double>& result) {
     compute_1e(Operator::nuclear(charges), result);
+  }
+  // H_core = T + V in one pass (Engine::compute_core_hamiltonian, engine.hpp:831-900).
+  void compute_core_hamiltonian(const PointChargeParams& charges, std::vector<double>& result) {
+    const std::size_t n = charges.n_centers();
+    if (charges.x.size() != n || charges.y.size() != n || charges.z.size() != n)
+      throw std::invalid_argument("compute_core_hamiltonian: PointChargeParams sizes differ");
+    std::vector<double> xyz, q(charges.charge);
+    for (std::size_t i = 0; i < n; ++i) xyz.insert(xyz.end(), {charges.x[i], charges.y[i], charges.z[i]});
+    result.assign(nbf_ * nbf_, 0.0);
+    check(lai_one_electron(h_, LAI_OP_HCORE, (int)n, xyz.empty() ? nullptr : xyz.data(),
+                           q.empty() ? nullptr : q.data(), result.data()),
+          "Engine::compute_core_hamiltonian");
   }
 
   // ---- work units (no Schwarz or primitive screening inside a unit) ----
@@ -598,6 +642,14 @@ inline void GpuFockBuilder::accumulate_device_eri_batch(Engine& engine, const do
                                            d_K_, stream_),
         "GpuFockBuilder::accumulate_device_eri_batch");
 }
+
+// The reference's namespace for its consumers (include/libaccint/consumers/).
+namespace consumers {
+using lai::FockBuilder;
+using lai::GpuFockBuilder;
+}  // namespace consumers
+
+using BackendHint = Engine::BackendHint;
 
 }  // namespace lai
 

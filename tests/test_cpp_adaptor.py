@@ -38,6 +38,31 @@ def test_one_electron_adaptor_compiles_and_links(tmp_path):
     assert exe.exists()
 
 
+def test_reference_style_usage_compiles_and_links(tmp_path):
+    """Code written with the reference's names (Shell(am, Point3D, ...), BasisSet({...}),
+    consumers::FockBuilder, BackendHint, compute_core_hamiltonian, Real/Size) builds."""
+    exe = tmp_path / "reference_style_usage"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), "-I",
+           "/usr/local/cuda/include", os.path.join(ROOT, "tests", "cpp", "reference_style_usage.cpp"), "-o",
+           str(exe), "-L", LIBDIR, "-laccint_b200", "-L", "/usr/local/cuda/lib64", "-lcudart",
+           "-Wl,-rpath," + LIBDIR, "-Wl,-rpath,/usr/local/cuda/lib64"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "warning" not in r.stderr, r.stderr
+
+
+@pytest.mark.gpu
+def test_reference_style_usage_runs(tmp_path):
+    """The same program on the device: H2 / STO-3G overlap S01 at 1.4 Bohr (0.6593, the
+    textbook value), a finite Fock element, and BackendHint::ForceCPU refused."""
+    test_reference_style_usage_compiles_and_links(tmp_path)
+    r = subprocess.run([str(tmp_path / "reference_style_usage")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    s01 = float(r.stdout.split("S01")[1].split()[0])
+    assert abs(s01 - 0.6593182061) < 1e-9
+    assert "ForceCPU refused: yes" in r.stdout
+
+
 @pytest.mark.gpu
 def test_adaptor_jk_matches_engine(tmp_path, lai):
     exe = _build(tmp_path)
