@@ -53,6 +53,14 @@ class ScreeningOptions:
     def loose():
         return ScreeningOptions(1e-10)
 
+    @staticmethod
+    def none():
+        """Every quartet (screening_options.hpp: threshold 0, disabled)."""
+        return ScreeningOptions(0.0, enabled=False)
+
+    def effective_threshold(self):
+        return self.threshold if self.enabled else 0.0
+
 
 class FockBuilder:
     """J/K accumulator (reference consumers::FockBuilder).  J and K accumulate
@@ -380,9 +388,7 @@ class Engine:
             raise RuntimeError("FockBuilder::accumulate called without density matrix")
         if consumer.nbf != self.basis.nbf:
             raise ValueError("FockBuilder nbf does not match the basis")
-        if screening is not None and screening.enabled and screening.threshold != self.threshold:
-            raise ValueError("screening threshold differs from the engine's; build an Engine "
-                             "with threshold=%g" % screening.threshold)
+        self._check_screening(screening)
         J, K, rep = self.jk(consumer.D)
         consumer.J += J
         consumer.K += K
@@ -390,6 +396,13 @@ class Engine:
 
     def compute(self, op, consumer):
         self.compute_and_consume(op, consumer)
+
+    def _check_screening(self, screening):
+        # the Schwarz cut is fixed when the engine is built (its pair lists depend on it)
+        if screening is not None and screening.effective_threshold() != self.threshold:
+            raise ValueError("screening threshold %g differs from the engine's %g; build an Engine "
+                             "with threshold=%g" % (screening.effective_threshold(), self.threshold,
+                                                    screening.effective_threshold()))
 
     def _consume_device(self, fb, screening):
         # device J/K of fb.d_D on torch's current stream of fb's device, added to
@@ -401,9 +414,7 @@ class Engine:
             raise ValueError("GpuFockBuilder nbf does not match the basis")
         if fb.device.index != self.device:
             raise ValueError(f"GpuFockBuilder is on cuda:{fb.device.index}, the engine on cuda:{self.device}")
-        if screening is not None and screening.enabled and screening.threshold != self.threshold:
-            raise ValueError("screening threshold differs from the engine's; build an Engine "
-                             "with threshold=%g" % screening.threshold)
+        self._check_screening(screening)
         J = torch.empty_like(fb.d_J)
         K = torch.empty_like(fb.d_K)
         stream = torch.cuda.current_stream(fb.device)

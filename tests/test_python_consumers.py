@@ -31,6 +31,44 @@ def test_operator_and_screening_mirrors(lai):
     assert lai.ScreeningOptions.normal().threshold == 1e-12
     assert lai.ScreeningOptions.tight().threshold == 1e-14
     assert lai.ScreeningOptions.loose().threshold == 1e-10
+    none = lai.ScreeningOptions.none()
+    assert not none.enabled and none.effective_threshold() == 0.0
+
+
+def _host_only_engine(lai, nbf, threshold):
+    # an Engine object without a device handle: enough for the argument checks,
+    # which all run before any device call
+    import types
+    eng = lai.Engine.__new__(lai.Engine)
+    eng._h = None
+    eng.basis = types.SimpleNamespace(nbf=nbf)
+    eng.threshold = threshold
+    eng.device = 0
+    return eng
+
+
+def test_compute_and_consume_argument_checks(lai):
+    n = 3
+    eng = _host_only_engine(lai, n, 1e-12)
+    op = lai.Operator.coulomb()
+    fb = lai.FockBuilder(n)
+    with pytest.raises(RuntimeError):           # density not set
+        eng.compute_and_consume(op, fb)
+    fb.set_density(np.eye(n))
+    with pytest.raises(ValueError):             # not a two-electron operator
+        eng.compute_and_consume(lai.engine.Operator("overlap"), fb)
+    with pytest.raises(ValueError):             # nbf mismatch
+        other = lai.FockBuilder(n + 1)
+        other.set_density(np.eye(n + 1))
+        eng.compute_and_consume(op, other)
+    # the Schwarz cut is the engine's: another threshold, or screening switched off
+    # (threshold 0), is refused rather than silently ignored
+    for scr in (lai.ScreeningOptions.tight(), lai.ScreeningOptions.none()):
+        with pytest.raises(ValueError):
+            eng.compute_and_consume(op, fb, scr)
+    eng0 = _host_only_engine(lai, n, 0.0)
+    eng0._check_screening(lai.ScreeningOptions.none())      # an unscreened engine accepts none()
+    eng._check_screening(lai.ScreeningOptions.normal())      # and the default engine normal()
 
 
 @pytest.mark.gpu
