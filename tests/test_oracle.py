@@ -69,3 +69,19 @@ def test_oracle_normalization_vs_reference(lai, oracle):
     b = lai.BasisSet.from_atoms(g["Z"], g["xyz"], "cc-pvqz")
     l, nprim, centers, exps, coefs = oracle.normalized_arrays(b)
     assert np.max(np.abs(coefs - g["coefs"])) < 1e-13 * np.max(np.abs(g["coefs"]))
+
+
+def test_reference_gpu_route_units_on_host(lai, oracle):
+    """Host side of the reference GPU harness (oracle/ref_gpu_shim.cu; built by
+    `make -C oracle refgpu`): the reference groups (H2O)8/STO-3G into its two ShellSets,
+    and the ordered set 4-tuples cover every ordered shell quartet exactly once.  No
+    device call is made here."""
+    if oracle.reference_gpu() is None:
+        pytest.skip("oracle/_ref/libref_gpu.so not built (make -C oracle refgpu)")
+    w = lai.workloads.make("h2o8_sto3g")
+    rb = oracle.RefGpuBasis(w.basis)
+    assert rb.nbf == w.nbf and rb.nsets == 2 and rb.nunits == 16
+    total = sum(rb.unit_size(u)[0] for u in range(rb.nunits))
+    assert total == w.basis.n_shells ** 4
+    with pytest.raises(ValueError):
+        rb.unit_size(rb.nunits)
