@@ -85,3 +85,16 @@ def test_reference_gpu_route_units_on_host(lai, oracle):
     assert total == w.basis.n_shells ** 4
     with pytest.raises(ValueError):
         rb.unit_size(rb.nunits)
+
+
+def test_oracle_jk_vs_reference_h2o_ccpvdz(lai, oracle):
+    """The restatement's J/K against the compiled reference's full Engine::compute path
+    for H2O / cc-pVDZ (s, p, d shells; up to 5 Rys roots), no screening."""
+    if oracle.reference() is None:
+        pytest.skip("oracle/_ref/libref_oracle.so not built")
+    w = lai.workloads.make("h2o1_ccpvdz")
+    J, K, nq = oracle.orc_jk(w.basis, w.D, 0.0)
+    Jr, Kr, _ = oracle.RefBasis(w.basis).jk_full(w.D)
+    assert nq == 3081  # every canonical quartet of 12 shells
+    assert np.max(np.abs(J - Jr)) < 1e-12
+    assert np.max(np.abs(K - Kr)) < 1e-12
