@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -34,6 +35,7 @@
 #include "engine_internal.h"
 #include "eri_kernels.h"
 #include "rys_tables.inc"
+#include "fp32_tables.h"
 
 namespace lai {
 void spherical_forget_basis(const lai_basis* basis);  // spherical.cu
@@ -248,6 +250,7 @@ void fill_pair_data(const lai_basis* basis, PairClassHost& c) {
   const int n = c.n();
   const int Kab = c.Ka * c.Kb;
   c.AB.assign(3 * (size_t)n, 0.0);
+  c.Acen.assign(3 * (size_t)n, 0.0);
   c.prim.assign((size_t)lai::PF_COUNT * Kab * n, 0.0);
   const double pi54s2 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
   for (int p = 0; p < n; ++p) {
@@ -258,6 +261,7 @@ void fill_pair_data(const lai_basis* basis, PairClassHost& c) {
       AB[x] = A.center[x] - B.center[x];
       ab2 += AB[x] * AB[x];
       c.AB[(size_t)x * n + p] = AB[x];
+      c.Acen[(size_t)x * n + p] = A.center[x];
     }
     for (int ia = 0; ia < c.Ka; ++ia)
       for (int ib = 0; ib < c.Kb; ++ib) {
@@ -284,6 +288,7 @@ int upload_class(PairClassHost& c) {
   LAI_CUDA_TRY(upload(c.d_fa, c.fa));
   LAI_CUDA_TRY(upload(c.d_fb, c.fb));
   LAI_CUDA_TRY(upload(c.d_AB, c.AB));
+  LAI_CUDA_TRY(upload(c.d_Acen, c.Acen));
   LAI_CUDA_TRY(upload(c.d_prim, c.prim));
   if (c.Q.empty()) c.Q.assign(c.n(), 0.0);
   LAI_CUDA_TRY(upload(c.d_Q, c.Q));
@@ -390,12 +395,16 @@ int compute_prim_schwarz(lai_engine* E) {
     pc.la = c.la; pc.lb = c.lb; pc.Ka = 1; pc.Kb = 1;
     pc.sa.resize(ne); pc.sb.resize(ne); pc.fa.resize(ne); pc.fb.resize(ne);
     pc.AB.resize(3 * (size_t)ne);
+    pc.Acen.resize(3 * (size_t)ne);
     pc.prim.assign((size_t)lai::PF_COUNT * ne, 0.0);
     for (int p = 0; p < n; ++p)
       for (int t = 0; t < Kab; ++t) {
         const int e = p * Kab + t;
         pc.sa[e] = c.sa[p]; pc.sb[e] = c.sb[p]; pc.fa[e] = c.fa[p]; pc.fb[e] = c.fb[p];
-        for (int x = 0; x < 3; ++x) pc.AB[(size_t)x * ne + e] = c.AB[(size_t)x * n + p];
+        for (int x = 0; x < 3; ++x) {
+          pc.AB[(size_t)x * ne + e] = c.AB[(size_t)x * n + p];
+          pc.Acen[(size_t)x * ne + e] = c.Acen[(size_t)x * n + p];
+        }
         for (int f = 0; f < lai::PF_COUNT; ++f)
           pc.prim[(size_t)f * ne + e] = c.prim[((size_t)f * Kab + t) * n + p];
       }
@@ -461,10 +470,14 @@ int sort_and_screen(lai_engine* E) {
       for (int i = 0; i < keep; ++i) o[i] = v[idx[i]];
       return o;
     };
-    std::vector<double> Q(keep), AB(3 * (size_t)keep), prim((size_t)lai::PF_COUNT * Kab * keep);
+    std::vector<double> Q(keep), AB(3 * (size_t)keep), Acen(3 * (size_t)keep),
+        prim((size_t)lai::PF_COUNT * Kab * keep);
     for (int i = 0; i < keep; ++i) {
       Q[i] = c.Q[idx[i]];
-      for (int x = 0; x < 3; ++x) AB[(size_t)x * keep + i] = c.AB[(size_t)x * n + idx[i]];
+      for (int x = 0; x < 3; ++x) {
+        AB[(size_t)x * keep + i] = c.AB[(size_t)x * n + idx[i]];
+        Acen[(size_t)x * keep + i] = c.Acen[(size_t)x * n + idx[i]];
+      }
       for (int f = 0; f < lai::PF_COUNT * Kab; ++f)
         prim[(size_t)f * keep + i] = c.prim[(size_t)f * n + idx[i]];
     }
@@ -484,7 +497,7 @@ int sort_and_screen(lai_engine* E) {
     }
     c.sa = perm(c.sa); c.sb = perm(c.sb); c.fa = perm(c.fa); c.fb = perm(c.fb);
     c.sys = perm(c.sys);
-    c.Q = std::move(Q); c.AB = std::move(AB); c.prim = std::move(prim);
+    c.Q = std::move(Q); c.AB = std::move(AB); c.Acen = std::move(Acen); c.prim = std::move(prim);
     c.seg.assign(E->nsys + 1, 0);
     for (int i = 0, s = 0; s <= E->nsys; ++s) {
       while (i < keep && c.sys[i] < s) ++i;
@@ -870,8 +883,14 @@ int create_engine(const lai_basis* basis, std::unique_ptr<lai_basis> merged, con
     LAI_CUDA_TRY(upload(E->d_hx2, hx));
     LAI_CUDA_TRY(upload(E->d_hw, hw));
     LAI_CUDA_TRY(upload(E->d_boys, bg));
+    // FP32 tables of the packed FP32 kernels, derived from the FP64 ones
+    std::vector<float> bf((size_t)lai::kBoysF32Rows * lai::kBoysF32Stride), rf(2 * (size_t)lai::kRysF32Len);
+    lai::build_boys_f32(BOYS_GRID_H, bf.data());
+    lai::build_rys_f32(RYS_COEF_H, rf.data());
+    LAI_CUDA_TRY(upload(E->d_boys_f32, bf));
+    LAI_CUDA_TRY(upload(E->d_rys_f32, rf));
     E->tab = {E->d_coef.as<double>(), E->d_hx2.as<double>(), E->d_hw.as<double>(),
-              E->d_boys.as<double>()};
+              E->d_boys.as<double>(), E->d_boys_f32.as<float>(), E->d_rys_f32.as<float>()};
   }
   if (int rc = build_classes(E.get())) return rc;
   for (auto& c : E->classes) {

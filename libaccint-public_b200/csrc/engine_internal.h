@@ -83,17 +83,19 @@ struct PairClassHost {
   std::vector<int> seg;             // [nsys + 1] first pair of each system (pairs sorted by system)
   std::vector<double> Q;
   std::vector<double> AB;          // SoA [3][n]
+  std::vector<double> Acen;        // SoA [3][n] centre of the first shell (a)
   std::vector<double> prim;        // SoA [PF_COUNT][Kab][n]
   int n() const { return (int)sa.size(); }
   // device copies
-  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_prim, d_sys, d_primf;
+  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_Acen, d_prim, d_sys, d_primf;
   bool batched = false;             // d_sys is set (more than one system)
   lai::PairClassDev view() const {
     lai::PairClassDev v;
     v.la = la; v.lb = lb; v.Ka = Ka; v.Kb = Kb; v.npairs = n();
     v.shell_a = d_sa.as<int>(); v.shell_b = d_sb.as<int>();
     v.func_a = d_fa.as<int>(); v.func_b = d_fb.as<int>();
-    v.Q = d_Q.as<double>(); v.AB = d_AB.as<double>(); v.prim = d_prim.as<double>();
+    v.Q = d_Q.as<double>(); v.AB = d_AB.as<double>(); v.Acen = d_Acen.as<double>();
+    v.prim = d_prim.as<double>();
     v.qprim_max = qprim_max;
     v.sys = batched ? d_sys.as<int>() : nullptr;
     v.primf = d_primf.as<float>();
@@ -117,6 +119,7 @@ struct ClassPairBlock {
   // qbegin32[p] its first ket).
   int64_t total64 = 0, total32 = 0;
   DevBuf d_off64, d_off32, d_qb32;
+
   lai::LaunchTune tune;         // launch parameters chosen by lai_engine_autotune (0 = heuristic)
 };
 
@@ -137,7 +140,7 @@ struct lai_engine {
   double thr = 1e-12;
   double prim_eps = 1e-15;
   cudaStream_t stream = nullptr;
-  lai::host::DevBuf d_coef, d_hx2, d_hw, d_boys;
+  lai::host::DevBuf d_coef, d_hx2, d_hw, d_boys, d_boys_f32, d_rys_f32;
   lai::RysTablesView tab{};
   std::vector<std::unique_ptr<lai::host::PairClassHost>> classes;
   std::vector<std::unique_ptr<lai::host::ClassPairBlock>> blocks;

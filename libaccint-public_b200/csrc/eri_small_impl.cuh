@@ -27,6 +27,7 @@
 #include "eri_device.cuh"
 #include "eri_kernels.h"
 #include "eri_tables_smem.cuh"
+#include "fp32_tables.h"
 
 namespace lai {
 
@@ -46,6 +47,25 @@ __device__ __forceinline__ T warp_sum(T v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// Compensated sum s + c (two-sum of Knuth: s' = s + x, z = s' - s,
+// c += (s - (s' - z)) + (x - z)).
+template <typename R>
+struct CompSum {
+  R s, c;
+};
+template <typename R>
+__device__ __forceinline__ void comp_add(CompSum<R>& a, R x) {
+  const R s1 = a.s + x;
+  const R z = s1 - a.s;
+  const R e = (a.s - (s1 - z)) + (x - z);
+  a.s = s1;
+  a.c += e;
+}
+
+template <int LA, int LB, int LC, int LD, typename GV>
+__device__ __forceinline__ void small_finish(GV&& gval, const QuartetBlock& blk, const JKArgs& args,
+                                             int64_t t, int p, int q, bool active, bool uniform_bra);
 
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>
 __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKArgs& args,
@@ -67,20 +87,44 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   const int Kcd = blk.ket.Ka * blk.ket.Kb;
   const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
 
+  constexpr bool F32 = sizeof(R) == 4;
+  // FP32: the primitive terms of one inner loop are summed in G, which is then
+  // added to the running total Gc with a compensated (two-sum) step (registers
+  // permitting: up to 18 (e0|f0) values); FP64: G is the total.
+  constexpr bool COMP = F32 && NE * NF <= 18;
   R G[NE * NF];
+  CompSum<R> Gc[COMP ? NE * NF : 1];
 #pragma unroll
   for (int i = 0; i < NE * NF; ++i) G[i] = R(0);
+#pragma unroll
+  for (int i = 0; i < (COMP ? NE * NF : 1); ++i) Gc[i].s = Gc[i].c = R(0);
+  auto merge = [&]() {
+    if constexpr (COMP) {
+#pragma unroll
+      for (int i = 0; i < NE * NF; ++i) {
+        comp_add(Gc[i], G[i]);
+        G[i] = R(0);
+      }
+    }
+  };
+  // FP32: P - Q = (A - C) + (P - A) - (Q - C) with A - C, the difference of the
+  // bra and ket pairs' first centres, formed in FP64, so that the error of P - Q
+  // scales with |P - A| rather than with the absolute coordinates.  FP64: P - Q
+  // from the stored centres P and Q (no extra registers held across the loop).
+  R AC[3];
+  if constexpr (F32) {
+#pragma unroll
+    for (int x = 0; x < 3; ++x)
+      AC[x] = R(__ldg(blk.bra.Acen + x * nbra + p) - __ldg(blk.ket.Acen + x * nket + q));
+  }
 
   const double peps = args.prim_eps;
   unsigned int nprim_done = 0;
   // unsplit: compile-time stride 1 keeps the bra loop warp-uniform
   const int ib0 = SPLIT ? sub : 0, ibs = SPLIT ? ps : 1;
-  // One primitive quartet: bra primitive pair (zeta, hz, P, PA, cab), ket
-  // primitive pair `cur`; accumulates into G.
-  // Pair data in the compute type: the FP32 kernels read an FP32 copy of the
-  // tables (half the bytes and registers, no conversions).  Their P - Q is then
-  // formed in FP32: an absolute error ~1e-7 |P| that moves T by ~1e-6 relative at
-  // worst, inside the FP32 error of the quartets the cut sends to this path.
+  // One primitive quartet: bra primitive pair (zeta, hz, PA, cab), ket
+  // primitive pair `cur`; accumulates into G.  The FP32 kernels read an FP32 copy
+  // of the pair tables (half the bytes and registers, no conversions).
   const R* __restrict__ bprim = prim_table<R>(blk.bra);
   const R* __restrict__ kprim = prim_table<R>(blk.ket);
   struct BraVals {
@@ -91,9 +135,11 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
     qab = __ldg(pb + PF_Q * sb);
     v.zeta = __ldg(pb + PF_ZETA * sb);
     v.hz = __ldg(pb + PF_HZ * sb);
-    v.Px = __ldg(pb + PF_PX * sb);
-    v.Py = __ldg(pb + PF_PY * sb);
-    v.Pz = __ldg(pb + PF_PZ * sb);
+    if constexpr (!F32) {
+      v.Px = __ldg(pb + PF_PX * sb);
+      v.Py = __ldg(pb + PF_PY * sb);
+      v.Pz = __ldg(pb + PF_PZ * sb);
+    }
     v.PAx = __ldg(pb + PF_PAX * sb);
     v.PAy = __ldg(pb + PF_PAY * sb);
     v.PAz = __ldg(pb + PF_PAZ * sb);
@@ -101,14 +147,13 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   };
   auto prim = [&](const BraVals& bv, const KetPrimT<R>& cur) {
     const R zeta = bv.zeta, hz = bv.hz, cab = bv.cab;
-    const R Px = bv.Px, Py = bv.Py, Pz = bv.Pz;
     const R PAx = bv.PAx, PAy = bv.PAy, PAz = bv.PAz;
     const R eta = R(cur.eta);
     const R he = R(cur.he);
-    const R PQx = Px - cur.px;
-    const R PQy = Py - cur.py;
-    const R PQz = Pz - cur.pz;
     const R QCx = R(cur.qcx), QCy = R(cur.qcy), QCz = R(cur.qcz);
+    const R PQx = F32 ? AC[0] + (PAx - QCx) : bv.Px - R(cur.px);
+    const R PQy = F32 ? AC[1] + (PAy - QCy) : bv.Py - R(cur.py);
+    const R PQz = F32 ? AC[2] + (PAz - QCz) : bv.Pz - R(cur.pz);
     const R ccd = R(cur.c);
     const R s = zeta + eta;
     const R rs = fast_rsqrt(s);
@@ -121,7 +166,7 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
       // -- the one-point Rys rule (w = F_0, u = F_1/F_0) written without its
       // quotient.
       R F0, F1;
-      boys01_smem<R>(T, stab, F0, F1);
+      if constexpr (F32) boys01_f32(T, stab, F0, F1); else boys01_smem<R>(T, stab, F0, F1);
       const R pw0 = pref * F0;
       if constexpr (LAB == 0) {
         G[0] += pw0;
@@ -139,7 +184,8 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
       return;
     }
     R u[NR], w[NR];
-    rys_smem<NR, R>(T, stab, tab, u, w);
+    if constexpr (F32) rys_f32(NR, T, stab, tab.herm_x2, tab.herm_w, u, w);
+    else rys_smem<NR, R>(T, stab, tab, u, w);
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       const R ur = u[r];
@@ -207,6 +253,7 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
         ++nprim_done;
         prim(bv, cur);
       }
+      merge();
     }
   } else {
     const R qket_max = R(blk.ket.qprim_max);
@@ -224,17 +271,40 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
         ++nprim_done;
         prim(bv, cur);
       }
+      merge();
     }
   }
 
   count_prims(args.prim_count, active ? nprim_done : 0u);
+  // contracted (e0|f0) values in FP64 (FP32: the compensated sum s + c)
+  double Gd[NE * NF];
+#pragma unroll
+  for (int i = 0; i < NE * NF; ++i) {
+    if constexpr (COMP) Gd[i] = double(Gc[i].s) + double(Gc[i].c);
+    else Gd[i] = double(G[i]);
+  }
   if (SPLIT) {
 #pragma unroll
     for (int i = 0; i < NE * NF; ++i)
-      for (int o = ps >> 1; o > 0; o >>= 1) G[i] += __shfl_xor_sync(0xffffffffu, G[i], o);
+      for (int o = ps >> 1; o > 0; o >>= 1) Gd[i] += __shfl_xor_sync(0xffffffffu, Gd[i], o);
     active = active && sub == 0;
   }
+  small_finish<LA, LB, LC, LD>([&](int i) { return Gd[i]; }, blk, args, t, p, q, active, uniform_bra);
+}
 
+// Horizontal transfer (closed form), normalization and the 8-fold symmetric
+// digestion of one contracted quartet (p, q), in double.  gval(i) returns the
+// contracted (e0|f0) integral i = e * NF + f.  Every lane of the warp must call
+// this together (the bra-pair Coulomb block is summed across the warp when
+// uniform_bra holds).
+template <int LA, int LB, int LC, int LD, typename GV>
+__device__ __forceinline__ void small_finish(GV&& gval, const QuartetBlock& blk, const JKArgs& args,
+                                             int64_t t, int p, int q, bool active, bool uniform_bra) {
+  constexpr int LAB = LA + LB, LCD = LC + LD;
+  constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  constexpr int NF = ncart_range(LC, LCD);
+  const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
+  (void)LAB;
   // ---- horizontal transfer (closed form) + normalization, in double ----
   const double ABx = __ldg(blk.bra.AB + p), ABy = __ldg(blk.bra.AB + nbra + p),
                ABz = __ldg(blk.bra.AB + 2 * nbra + p);
@@ -273,7 +343,7 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
             const double cf = bc * abp[0][comp_x(cb) - kx] * abp[1][comp_y(cb) - ky] *
                               abp[2][comp_z(cb) - kz];
 #pragma unroll
-            for (int f = 0; f < NF; ++f) H[(a * NB + b) * NF + f] += cf * double(G[row * NF + f]);
+            for (int f = 0; f < NF; ++f) H[(a * NB + b) * NF + f] += cf * gval(row * NF + f);
           });
         });
       });
@@ -473,12 +543,12 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
 // 65536 / (256 * blocks)).  The light classes are latency bound with short
 // dependent chains and need the warps: in FP64 (ss|ss) fits 64 registers (4
 // blocks, 32 warps) and (ps|ss) 80 (3 blocks); in FP32 the one-root classes fit 64
-// and the L = 2 ones 80.  The other classes keep ptxas's own choice (0 = no bound;
+// and the L = 2 ones, with their compensated accumulators, 128 (2 blocks).  The other classes keep ptxas's own choice (0 = no bound;
 // an explicit 1 would let it take up to 255 registers).
 template <int LA, int LB, int LC, int LD, typename R>
 __host__ __device__ constexpr int small_min_blocks() {
   constexpr int L = LA + LB + LC + LD;
-  return sizeof(R) == 8 ? (L == 0 ? 4 : L == 1 ? 3 : 0) : (L <= 1 ? 4 : L == 2 ? 3 : 0);
+  return sizeof(R) == 8 ? (L == 0 ? 4 : L == 1 ? 3 : 0) : (L <= 1 ? 4 : L == 2 ? 2 : 0);
 }
 
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>
@@ -487,7 +557,8 @@ __global__ void __launch_bounds__(256, (small_min_blocks<LA, LB, LC, LD, R>()))
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* stab = reinterpret_cast<R*>(smem_raw);
-  stage_table<NR, R>(stab, tab);
+  if constexpr (sizeof(R) == 4) stage_table_f32<NR>(reinterpret_cast<float*>(smem_raw), tab);
+  else stage_table<NR, R>(stab, tab);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   if (!SPLIT) ps = 1;
@@ -533,7 +604,7 @@ int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView&
                cudaStream_t stream, bool fp32, int num_sms, LaunchTune tune) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
   const int threads = 256;
-  const size_t smem = fp32 ? table_bytes<NR, float>() : table_bytes<NR, double>();
+  const size_t smem = fp32 ? f32_table_bytes<NR>() : table_bytes<NR, double>();
   const int64_t nq = blk.total - blk.t_begin;
   if (nq <= 0) return 1;
   // lanes per quartet: split the bra primitive loop when the launch has too few

@@ -51,6 +51,7 @@ struct PairClassDev {
   const int* func_b;   // [npairs]
   const double* Q;     // [npairs] Schwarz bound, descending
   const double* AB;    // [3 * npairs] A - B, SoA
+  const double* Acen;  // [3 * npairs] centre A of the first shell, SoA
   const double* prim;  // [PF_COUNT * Ka*Kb * npairs]
   double qprim_max;    // largest PF_Q of the class
   const int* sys;      // [npairs] system of each pair in a batched engine, else nullptr
