@@ -1,7 +1,8 @@
 """Build ``basis_sets.json`` (the basis-set data this package ships) from the
 reference's bundled Basis Set Exchange files and its built-in STO-3G table.
 
-Run in a checkout that has the reference tree (default /root/reference):
+Run in a checkout that has the reference tree (argument, else the environment
+variable LIBACCINT_REFERENCE, else the default in main()):
 
     python make_basis_data.py [REFERENCE_ROOT]
 
@@ -76,7 +77,7 @@ def parse_builtin_aux(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LIBACCINT_REFERENCE", "/root/reference")
     data = {}
     for name in BSE_FILES:
         j = json.load(open(os.path.join(ref, "share", "basis_sets", name + ".json")))

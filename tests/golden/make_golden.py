@@ -13,8 +13,10 @@ Fixtures and their provenance:
                          test_water_cluster_validation.cpp:454-495.
 * <workload>_ref.npz  -- J/K of the UNMODIFIED reference, Engine::compute(coulomb,
                          FockBuilder) (full N^4, no screening), for the seeded
-                         workloads h2o8_sto3g (config 0: built-in STO-3G, 8 waters)
-                         and h2o2_ccpvdz, plus the density used.
+                         workloads h2o8_sto3g (config 0: built-in STO-3G, 8 waters),
+                         h2o2_ccpvdz and h2o1_ccpvqz (s..g shells, every class up
+                         to (gg|gg); about 150 s on 8 cores, option "refqz"), plus
+                         the density used.
 * one_electron_sto3g.npz -- tests/integration/test_one_electron.cpp of the reference
                          (PySCF cart=True values written into the test): the H2 and
                          H2O STO-3G shells, point charges and S, T, V matrices; and
@@ -35,7 +37,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+# reference checkout: argument, else $LIBACCINT_REFERENCE, else the default below
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LIBACCINT_REFERENCE", "/root/reference")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle  # noqa: E402
@@ -220,5 +223,7 @@ if __name__ == "__main__":
         ref_jk("h2o2_sto3g")
         ref_jk("h2o2_ccpvdz")
         norm_ccpvqz()
+    if "refqz" in only:
+        ref_jk("h2o1_ccpvqz")
     if "eri" in only:
         eri_samples()

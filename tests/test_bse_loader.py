@@ -10,7 +10,8 @@ import os
 import numpy as np
 import pytest
 
-REF_SHARE = "/root/reference/share/basis_sets"
+# the reference checkout ($LIBACCINT_REFERENCE, else the default below), when present
+REF_SHARE = os.path.join(os.environ.get("LIBACCINT_REFERENCE", "/root/reference"), "share", "basis_sets")
 
 
 def _shells(b):
