@@ -164,6 +164,16 @@ def time_reference(R, cq, D, target_s, seed, nthreads=0):
     return n / t, n, t
 
 
+def jk_config(args, w, total_q, ws, **extra):
+    """The config block both arms print (identically) for a single-system J/K workload."""
+    cfg = {"workload": args.workload, "system": SYSTEMS.get(args.workload, args.workload),
+           "nbf": w.nbf, "shells": w.basis.n_shells, "quartets": int(total_q), "schwarz": w.thr,
+           "nocc": w.nocc, "parallelism": f"quartet shards x{ws}" + (" + NCCL all-reduce" if ws > 1 else ""),
+           "l2": "GPU arm: L2 flushed (256 MB write) between timed steps"}
+    cfg.update(extra)
+    return cfg
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -180,26 +190,30 @@ def run_reference(args):
         return 0
     R, cq = s
     cores = host_cores()
+    # every step is one fixed-size sample of the canonical quartets, sized in the
+    # warm-up to about step_target seconds on all host cores
     step_target = max(2.0, args.cpu_seconds / 2)
+    rate0, _, _ = time_reference(R, cq, w.D, step_target / 4, 1000)
+    n_step = int(min(max(rate0 * step_target, 1000), 5e7))
     for i in range(args.warmup):
-        time_reference(R, cq, w.D, step_target / 4, 1000 + i)
-    rates, ns, ts = [], 0, 0.0
+        R.time_quartets(w.D, cq.sample(max(1000, n_step // 4), 1100 + i), 0)
+    walls, kern = [], []
     for i in range(args.steps):
-        r, n, t = time_reference(R, cq, w.D, step_target, 2000 + 17 * i)
-        rates.append(r)
-        ns += n
-        ts += t
-    value = ns / ts
-    sample = (f"{ns} canonical quartets drawn uniformly (seeded) from the {cq.total} of "
-              f"{args.workload} over {args.steps} steps; compute_2e_shell_quartet + "
-              f"accumulate_symmetric, OpenMP {cores} threads")
+        smp = cq.sample(n_step, 2000 + 17 * i)
+        t0 = time.perf_counter()
+        kern.append(R.time_quartets(w.D, smp, 0)[0])
+        walls.append(time.perf_counter() - t0)
+    value = n_step * args.steps / sum(kern)
+    sample = (f"{n_step} canonical quartets per step drawn uniformly (seeded) from the {cq.total} of "
+              f"{args.workload}; compute_2e_shell_quartet + accumulate_symmetric, OpenMP {cores} threads")
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * cq.total / value, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls), "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": args.workload, "quartets": cq.total, "nbf": w.nbf, "schwarz": w.thr,
-                   "l2": "inputs larger than L2 (J/K scattered over 20 MB x 3, pair data ~0.4 GB)"},
+        "config": jk_config(args, w, cq.total, ws),
+        "schedule": "reference CPU path (OpenMP, all host cores)",
+        "quartets_per_step": n_step,
         "jk_build_s": cq.total / value, "jk_build_s_kind": "extrapolated from the sample",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -464,16 +478,16 @@ def mixed_leg(eng, D, J64, K64, flush, stream, steps, fp64_ms, cut=MIXED_CUT):
         torch.cuda.synchronize()
         ms.append(a.elapsed_time(b))
 
-    def energy(J, K):
-        return float(0.5 * torch.sum(D * J).item() - 0.25 * torch.sum(D * K).item())
-
+    # dE = tr(D dJ)/2 - tr(D dK)/4 from the differences themselves: differencing two
+    # energies of ~4.5e3 Eh would bottom out at their rounding (~1e-12 Eh)
+    dE = float(0.5 * torch.sum(D * (Jm - J64)).item() - 0.25 * torch.sum(D * (Km - K64)).item())
     m = sum(ms) / len(ms)
     n32, n64 = int(rep.quartets_fp32), int(rep.quartets_fp64)
     return {"fp32_cut": cut, "ms_per_build": m, "speedup_vs_fp64": fp64_ms / m,
             "quartets_fp32": n32, "quartets_fp64": n64, "fp32_fraction": n32 / max(1, n32 + n64),
             "max_abs_dJ": float(torch.max(torch.abs(Jm - J64)).item()),
             "max_abs_dK": float(torch.max(torch.abs(Km - K64)).item()),
-            "abs_dE": abs(energy(Jm, Km) - energy(J64, K64)),
+            "abs_dE": abs(dE), "dE": dE,
             "bar": "|dE| < 1e-8 Eh against the FP64 build"}
 
 
@@ -642,12 +656,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "system": SYSTEMS.get(args.workload, args.workload),
-                       "nbf": n, "shells": w.basis.n_shells, "quartets": total_q, "schwarz": w.thr,
-                       "nocc": w.nocc, "parallelism": f"quartet shards x{ws}" + (" + NCCL all-reduce" if ws > 1 else ""),
-                       "l2": "flushed (256 MB write) between timed steps",
-                       "schedule": "autotuned in the set-up (lai_engine_autotune)" if tune else
-                                   "built-in launch heuristics"},
+            "config": jk_config(args, w, total_q, ws),
+            "schedule": "autotuned in the set-up (lai_engine_autotune)" if tune else "built-in launch heuristics",
             "jk_build_s": ms_per_step * 1e-3,
             "energy": E, "energy_e2e": E2,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n * n,
