@@ -169,10 +169,10 @@ LAI_API int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d
                         void* stream, const lai_jk_opts* opts, lai_jk_report* report);
 
 /* J/K build that allocates nothing when called (no counterpart in the
- * reference).  For callers that cannot call cudaMalloc at this point: code
- * recording a CUDA graph, plugins whose host application owns the whole device
- * through its own allocator, real-time drivers that forbid allocation after
- * start-up.  Same result as lai_jk_build_device(); the two nbf x nbf
+ * reference).  For callers that cannot call cudaMalloc at this point: plugins
+ * whose host application owns the whole device through its own allocator, and
+ * real-time drivers that forbid allocation after start-up (an allocation can
+ * synchronize the device).  Same result as lai_jk_build_device(); the two nbf x nbf
  * accumulators live in a fixed 4 MiB array of the library's device image
  * (held on every GPU that loads the library until exit), hence
  * nbf <= LAI_NOALLOC_MAX_NBF, else LAI_EINVAL.  All calls share the

@@ -1,10 +1,10 @@
 // J/K build that performs no device allocation at call time.
 //
 // Who needs it: hosts that cannot call cudaMalloc when they ask for J and K --
-// code recording a CUDA graph (allocation is not allowed while a stream is being
-// captured), plugins living in an application that reserves the whole device up
-// front for its own pool allocator, and real-time drivers that forbid allocation
-// once initialised.  lai_jk_build_device() allocates its two nbf x nbf
+// plugins living in an application that reserves the whole device up front for
+// its own pool allocator (a cudaMalloc there fails or steals the pool's memory),
+// and real-time drivers that forbid allocation once initialised (an allocation
+// can synchronize the device and take unbounded time).  lai_jk_build_device() allocates its two nbf x nbf
 // accumulators on first use; this variant keeps them instead in a fixed array in
 // the library's device image, so the call itself allocates nothing.  The caller
 // still owns D, J and K, and the engine (created earlier with lai_engine_create,
@@ -20,6 +20,7 @@
 //     stream capture.
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <mutex>
 
 #include "../../include/libaccint_b200.h"
@@ -107,11 +108,22 @@ extern "C" int lai_jk_build_noalloc(lai_engine* engine, const double* d_D, doubl
     const int la = q.bra.la, lb = q.bra.lb, lc = q.ket.la, ld = q.ket.lb;
     int rc;
     if (lai::small_class_supported(la, lb, lc, ld))
-      rc = lai::launch_small(q, args, tab, s, false, sms) == 1 ? 0 : -1;
+      rc = lai::launch_small(q, args, tab, s, false, sms) == 1 ? 0 : -3;
     else if (lai::sliced_class_supported(la, lb, lc, ld))
-      rc = lai::launch_sliced(q, args, tab, s, false, sms) == 1 ? 0 : -1;
+      rc = lai::launch_sliced(q, args, tab, s, false, sms) == 1 ? 0 : -3;
     else
       rc = lai::launch_tiled(q, args, tab, s, sms);
+    if (rc == -1) {  // launch_tiled only
+      // the tiled kernel's shared-memory tables do not fit this class; the
+      // allocating entry point would fall back to the generic kernel, which needs
+      // global scratch memory
+      char msg[160];
+      snprintf(msg, sizeof msg,
+               "lai_jk_build_noalloc: class (%c%c|%c%c) does not fit the tiled kernel's shared "
+               "memory; use lai_jk_build_device", "spdfghik"[la], "spdfghik"[lb], "spdfghik"[lc],
+               "spdfghik"[ld]);
+      return err(LAI_ENOTSUP, msg);
+    }
     if (rc < 0) return err(LAI_ECUDA, "lai_jk_build_noalloc: kernel launch failed");
   }
   if (nn > 0)
