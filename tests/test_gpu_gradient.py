@@ -98,6 +98,94 @@ def test_autograd_function(lai):
     assert abs((ep - em) / 2e-5 - np.sum(D.grad.numpy() * X)) < 1e-6
 
 
+
+def test_autograd_mixed_forward_vs_finite_differences(lai):
+    """Config 4's mixed-precision variant on (H2O)2 / cc-pVDZ: the forward in mixed
+    precision (FP32 below Q_ij Q_kl max|D| = 1e-7), the gradient of every
+    coordinate against central differences (h = 1e-4) of that same mixed forward,
+    and the mixed energy against the FP64 one (bar 1e-8 Eh)."""
+    import torch
+    w = lai.workloads.make("h2o2_ccpvdz")
+    dev = torch.device("cuda", 0)
+    D = torch.tensor(w.D, dtype=torch.float64, device=dev)
+    cut = 1e-7
+
+    def e_mixed(xyz):
+        R = torch.tensor(xyz, dtype=torch.float64)
+        return lai.autograd.jk_energy(R, D, w.Z, "cc-pvdz", 0.0, 0.0, cut).item()
+
+    R = torch.tensor(w.xyz, dtype=torch.float64, requires_grad=True)
+    E = lai.autograd.jk_energy(R, D, w.Z, "cc-pvdz", 0.0, 0.0, cut)
+    E.backward()
+    E64 = lai.autograd.jk_energy(torch.tensor(w.xyz, dtype=torch.float64), D, w.Z, "cc-pvdz", 0.0, 0.0)
+    assert abs(E.item() - E64.item()) < 1e-8
+    g = R.grad.numpy()
+    fd = np.zeros_like(g)
+    for a in range(len(w.Z)):
+        for x in range(3):
+            xp = w.xyz.copy(); xp[a, x] += H
+            xm = w.xyz.copy(); xm[a, x] -= H
+            fd[a, x] = (e_mixed(xp) - e_mixed(xm)) / (2 * H)
+    assert np.max(np.abs(g - fd)) < GRAD_TOL, np.max(np.abs(g - fd))
+
+
+def test_autograd_device_tensors_and_engine_cache(lai):
+    """CUDA tensors in, CUDA gradients out; a second density at the same geometry
+    reuses the cached engine; a moved geometry rebuilds it."""
+    import torch
+    w = lai.workloads.make("h2o2_sto3g")
+    dev = torch.device("cuda", 0)
+    R = torch.tensor(w.xyz, dtype=torch.float64, device=dev, requires_grad=True)
+    D = torch.tensor(w.D, dtype=torch.float64, device=dev, requires_grad=True)
+    E = lai.autograd.jk_energy(R, D, w.Z, "sto-3g", 0.0, 0.0)
+    E.backward()
+    assert R.grad.is_cuda and D.grad.is_cuda and E.is_cuda
+    eng = lai.autograd._engines.eng
+    b = lai.BasisSet.from_atoms(w.Z, w.xyz, "sto-3g")
+    e = lai.Engine(b, threshold=0.0, prim_threshold=0.0)
+    assert np.max(np.abs(R.grad.cpu().numpy() - e.gradient(w.D))) < 1e-12
+    lai.autograd.jk_energy(R.detach(), 2.0 * D.detach(), w.Z, "sto-3g", 0.0, 0.0)
+    assert lai.autograd._engines.eng is eng
+    lai.autograd.jk_energy(R.detach() + 0.01, D.detach(), w.Z, "sto-3g", 0.0, 0.0)
+    assert lai.autograd._engines.eng is not eng
+
+
+def test_gradient_h2o16_device_time(lai):
+    """Config 4 (H2O)16 / cc-pVDZ, Schwarz 1e-12: device time of the J/K build and
+    of the gradient kernel (CUDA events, after a warm-up), printed for the record."""
+    import torch
+    w = lai.workloads.make("h2o16_ccpvdz")
+    e = lai.Engine(w.basis, threshold=1e-12)
+    dev = torch.device("cuda", 0)
+    D = torch.tensor(w.D, dtype=torch.float64, device=dev)
+    J = torch.empty_like(D)
+    K = torch.empty_like(D)
+    G = torch.empty((e.natom(), 3), dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream()
+    import ctypes
+
+    def grad():
+        lai._lib.check(lai.lib().lai_jk_gradient_device(e._h, ctypes.c_void_p(D.data_ptr()),
+                                                         ctypes.c_void_p(G.data_ptr()),
+                                                         ctypes.c_void_p(s.cuda_stream)))
+
+    def jk():
+        e.jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr(), stream=s.cuda_stream)
+
+    out = {}
+    for name, f in (("jk", jk), ("gradient", grad)):
+        f()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(3):
+            f()
+        b.record(s)
+        torch.cuda.synchronize()
+        out[name] = a.elapsed_time(b) / 3
+    print(f"(H2O)16/cc-pVDZ: J/K build {out['jk']:.2f} ms, gradient {out['gradient']:.2f} ms")
+    assert np.max(np.abs(G.sum(dim=0).cpu().numpy())) < 1e-8
+
 def test_gradient_requires_atoms(lai):
     w = lai.workloads.make("h2o1_sto3g")
     shells = [lai.Shell(s.l, s.center, s.exps, s.coefs) for s in w.basis.shells]  # atom = -1
