@@ -14,8 +14,10 @@ Three- and two-centre integrals come from the device kernels of
 libaccint_b200.so (lai_eri3c_device / lai_eri2c_device); the metric
 factorization, the triangular solve and the contractions are FP64 cuBLAS /
 cuSOLVER calls through torch on tensors resident in HBM: K runs as one batched
-GEMM over the auxiliary index after factoring D = C+ C+^T - C- C-^T (symmetric
-eigendecomposition), and one large GEMM.
+GEMM over the auxiliary index and one large GEMM on the factors of D: the
+orbitals given to set_orbitals (D = w C C^T, nothing to factor), or else
+D = C+ C+^T - C- C-^T from one symmetric eigendecomposition per density
+(cached until the next set_density).
 
 The reference forms B = T L^-1 (three_center_eri_kernel.cpp:364-387 with L_inv from
 math::triangular_inverse), which is the fitted (ab|cd) only if L^T L = L L^T; and
@@ -52,6 +54,7 @@ class DFFockBuilder:
         self.dev = torch.device("cuda", engine.device)
         self.BT = None        # (naux, n, n): B^P matrices, contiguous per P
         self.D = None
+        self._factors = None
         self.J = None
         self.K = None
         self.init_ms = None
@@ -89,6 +92,37 @@ class DFFockBuilder:
         if Dt.shape != (self.n, self.n):
             raise ValueError(f"density must be {self.n}x{self.n}")
         self.D = Dt
+        self._factors = None  # factored on the first exchange build of this density
+
+    def set_orbitals(self, C, weight=1.0):
+        """The density as D = weight * C C^T from (nbf, m) orbital coefficients, e.g.
+        the occupied orbitals of an SCF step with weight 2.  The exchange build then
+        contracts with C directly and factors nothing."""
+        torch = _torch()
+        Ct = torch.as_tensor(C, dtype=torch.float64).to(self.dev)
+        if Ct.dim() != 2 or Ct.shape[0] != self.n:
+            raise ValueError(f"orbitals must be {self.n} x m")
+        if not weight > 0.0:
+            raise ValueError("set_orbitals: weight must be positive")
+        self.D = weight * (Ct @ Ct.T)
+        self._factors = [(1.0, Ct * (weight ** 0.5))]
+
+    def _factor_density(self):
+        """D = sum_s s C_s C_s^T (s = +1, -1) from the symmetric eigendecomposition,
+        once per density."""
+        torch = _torch()
+        if getattr(self, "_factors", None) is not None:
+            return self._factors
+        Ds = 0.5 * (self.D + self.D.T)
+        lam, U = torch.linalg.eigh(Ds)
+        scale = torch.max(torch.abs(lam)) if lam.numel() else torch.tensor(0.0)
+        out = []
+        for sign in (1.0, -1.0):
+            keep = sign * lam > self.eig_cut * scale
+            if bool(torch.any(keep)):
+                out.append((sign, U[:, keep] * torch.sqrt(sign * lam[keep])))
+        self._factors = out
+        return out
 
     def _need(self):
         if self.D is None:
@@ -107,15 +141,8 @@ class DFFockBuilder:
         self._need()
         torch = _torch()
         n, naux = self.n, self.naux
-        Ds = 0.5 * (self.D + self.D.T)
-        lam, U = torch.linalg.eigh(Ds)
-        scale = torch.max(torch.abs(lam)) if lam.numel() else torch.tensor(0.0)
         K = torch.zeros((n, n), dtype=torch.float64, device=self.dev)
-        for sign in (1.0, -1.0):
-            keep = sign * lam > self.eig_cut * scale
-            if not bool(torch.any(keep)):
-                continue
-            C = U[:, keep] * torch.sqrt(sign * lam[keep])
+        for sign, C in self._factor_density():
             X = torch.matmul(self.BT, C)                       # (naux, n, m)
             Xf = X.permute(1, 0, 2).reshape(n, -1)             # (n, naux*m)
             K = K + sign * (Xf @ Xf.T)

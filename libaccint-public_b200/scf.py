@@ -93,9 +93,12 @@ class RHF:
             from .df import DFFockBuilder
             self.df = DFFockBuilder(self.engine, aux)
 
-    def _jk(self, D, J, K, stream):
+    def _jk(self, D, J, K, stream, Cocc=None):
         if self.df is not None:
-            self.df.set_density(D)
+            if Cocc is not None:  # D = 2 Cocc Cocc^T: the exchange contracts with Cocc, no factoring
+                self.df.set_orbitals(Cocc, 2.0)
+            else:
+                self.df.set_density(D)
             J.copy_(self.df.compute_coulomb())
             K.copy_(self.df.compute_exchange())
             return
@@ -132,6 +135,7 @@ class RHF:
 
             _, C = solve(H)
             D = density(C)
+            Cocc = C[:, :self.nocc]
             J = torch.empty_like(S)
             K = torch.empty_like(S)
             one_e_ms = e0.elapsed_time(e1)
@@ -143,7 +147,7 @@ class RHF:
             for it in range(max_iterations):
                 a, b, c = ev(), ev(), ev()
                 a.record(stream)
-                self._jk(D, J, K, stream)
+                self._jk(D, J, K, stream, Cocc)
                 b.record(stream)
                 F = H + J - 0.5 * K
                 E = 0.5 * float(torch.sum((H + F) * D)) + self.e_nuc
@@ -168,6 +172,7 @@ class RHF:
                     Fd = sum(float(coef[i]) * fock_hist[i] for i in range(m))
                 eps, C = solve(Fd)
                 Dn = density(C)
+                Cn = C[:, :self.nocc]
                 dD = float(torch.max(torch.abs(Dn - D)))
                 c.record(stream)
                 c.synchronize()
@@ -175,15 +180,15 @@ class RHF:
                 iter_ms.append(a.elapsed_time(c))
                 energies.append(E)
                 if abs(E - E_old) < energy_threshold and dD < density_threshold and it > 0:
-                    D = Dn
+                    D, Cocc = Dn, Cn
                     converged = True
                     break
-                D = Dn
+                D, Cocc = Dn, Cn
                 E_old = E
             if converged:
                 a, b = ev(), ev()
                 a.record(stream)
-                self._jk(D, J, K, stream)
+                self._jk(D, J, K, stream, Cocc)
                 b.record(stream)
                 F = H + J - 0.5 * K
                 E_final = 0.5 * float(torch.sum((H + F) * D)) + self.e_nuc

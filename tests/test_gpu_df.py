@@ -64,6 +64,29 @@ def test_df_jk_matches_numpy_fitting(lai, oracle):
     assert torch.is_tensor(df.get_coulomb_matrix())
 
 
+
+def test_df_exchange_from_orbitals(lai):
+    """set_orbitals(C, w): D = w C C^T and K built from C directly (no factoring of
+    D) equal the set_density build of the same D; a second exchange build at the
+    same density reuses its factors and gives the same K."""
+    import torch
+    w = lai.workloads.make("h2o2_ccpvdz")
+    aux = lai.BasisSet.from_atoms(w.Z, w.xyz, "cc-pvdz-ri")
+    eng = lai.Engine(w.basis)
+    rng = np.random.default_rng(5)
+    C = rng.standard_normal((w.nbf, 10)) / np.sqrt(w.nbf)
+    df = lai.df.DFFockBuilder(eng, aux)
+    df.set_orbitals(C, 2.0)
+    Jo, Ko = df.compute_coulomb().cpu().numpy(), df.compute_exchange().cpu().numpy()
+    df.set_density(2.0 * C @ C.T)
+    Jd, Kd = df.compute_coulomb().cpu().numpy(), df.compute_exchange().cpu().numpy()
+    assert np.max(np.abs(Jo - Jd)) < 1e-12
+    assert np.max(np.abs(Ko - Kd)) < 1e-11
+    K2 = df.compute_exchange().cpu().numpy()
+    assert np.array_equal(K2, Kd)
+    with pytest.raises(ValueError):
+        df.set_orbitals(torch.zeros((w.nbf + 1, 3)), 1.0)
+
 def test_df_rhf_close_to_four_center(lai):
     w = lai.workloads.make("h2o2_ccpvdz")
     aux = lai.BasisSet.from_atoms(w.Z, w.xyz, "cc-pvdz-ri")
