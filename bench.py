@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target CPU time of the reference sample (per step for --impl reference)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (0, 2, 3, 4) timed after the headline workload")
     ap.add_argument("--no-autotune", action="store_true",
                     help="J/K workloads: skip lai_engine_autotune in the set-up (built-in launch heuristics)")
     return ap.parse_args()
@@ -408,21 +410,38 @@ def run_df(args):
     df.initialize()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     s = torch.cuda.current_stream()
+    # the occupied orbitals of the synthetic density (D = C C^T, rank nocc), as an
+    # SCF step hands them over; factored once on the host, outside the timing
+    lam, U = np.linalg.eigh(w.D)
+    C = torch.from_numpy(U[:, -w.nocc:] * np.sqrt(np.maximum(lam[-w.nocc:], 0.0))).to(dev)
+
+    def step(orbitals):
+        # one SCF step's J and K: a new density each time (its factors are not reused)
+        if orbitals:
+            df.set_orbitals(C, 1.0)
+        else:
+            df.set_density(D)
+        return df.compute_coulomb(), df.compute_exchange()
+
+    def timed(orbitals, n):
+        ms = []
+        for _ in range(n):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            JK = step(orbitals)
+            b.record(s)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return ms, JK
+
     for _ in range(args.warmup):
-        df.compute_coulomb()
-        df.compute_exchange()
+        step(True)
+        step(False)
     torch.cuda.synchronize()
     clk = ClockSampler(local)
-    ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(s)
-        J = df.compute_coulomb()
-        K = df.compute_exchange()
-        b.record(s)
-        torch.cuda.synchronize()
-        ms.append(a.elapsed_time(b))
+    ms, (J, K) = timed(True, args.steps)
+    ms_d, _ = timed(False, args.steps)
     clk = clk.stop()
     E = lai.molecules.energy(w.D, J.cpu().numpy(), K.cpu().numpy())
     # the exact four-centre build of the same density, for the fitting error and the time
@@ -444,6 +463,9 @@ def run_df(args):
         "config": {"workload": args.workload, "system": SYSTEMS.get(name, name), "nbf": w.nbf,
                    "aux": "cc-pVDZ-RI (built-in set of the reference)", "naux": aux.nbf,
                    "l2": "flushed (256 MB write) between timed steps"},
+        "step": "set_orbitals(C_occ) + compute_coulomb + compute_exchange (a new density each step)",
+        "density_path_ms": statistics.mean(ms_d),
+        "density_path": "set_density(D) + J + K: D factored by one eigendecomposition per step",
         "setup_ms": df.init_ms, "energy": E, "energy_four_center": E4, "fitting_error": E - E4,
         "four_center_jk_ms": a.elapsed_time(b),
         "clocks": clk,
@@ -490,6 +512,136 @@ def mixed_leg(eng, D, J64, K64, flush, stream, steps, fp64_ms, cut=MIXED_CUT):
             "abs_dE": abs(dE), "dE": dE,
             "bar": "|dE| < 1e-8 Eh against the FP64 build"}
 
+
+
+def _device_ms(fn, flush, stream, steps):
+    """Mean device time (ms) of fn() over `steps` calls after one warm-up call:
+    CUDA events on `stream`, L2 flushed before each call (outside the events)."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    return statistics.mean(ms)
+
+
+def side_configs(lai, dev, flush, stream, steps, cpu_baseline=True):
+    """The other configurations of the benchmark set, each timed once in the default
+    run (device time per build, L2 flushed; one GPU): config 0 against the reference's
+    own CPU FockBuilder build in full, config 2 (C12H26/cc-pVTZ) plain FP64 and mixed,
+    config 3 (256 clusters, batched engine, CUDA graph) plain FP64 and mixed, config 4
+    (the (H2O)16 nuclear gradient)."""
+    import ctypes
+    import torch
+    s = stream.cuda_stream
+    out = {}
+
+    def dev_mats(n):
+        return (torch.empty((n, n), dtype=torch.float64, device=dev),
+                torch.empty((n, n), dtype=torch.float64, device=dev))
+
+    # config 0: (H2O)8 / STO-3G, plain FP64
+    w = lai.workloads.make("h2o8_sto3g")
+    eng = lai.Engine(w.basis, threshold=w.thr, device=dev.index)
+    D = torch.from_numpy(w.D).to(dev)
+    J, K = dev_mats(w.nbf)
+    ms = _device_ms(lambda: eng.jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr(), stream=s), flush, stream, steps)
+    nq = eng.quartet_count()
+    c0 = {"system": SYSTEMS["h2o8_sto3g"], "nbf": w.nbf, "quartets": nq, "schwarz": w.thr, "dtype": "f64",
+          "ms_per_build": ms, "quartets_per_s": nq / (ms * 1e-3)}
+    if cpu_baseline:
+        # the reference's own CPU path in full: Engine::compute(coulomb, FockBuilder),
+        # N^4 without screening, OpenMP on all host cores (oracle/_ref)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        if oracle.reference() is not None:
+            R = oracle.RefBasis(builtin_sto3g=(w.Z, w.xyz))
+            Jr, Kr, t = R.jk_full(w.D, 0)
+            c0["cpu_baseline"] = {"kind": "reference", "cores": host_cores(), "full_build_s": t,
+                                  "sample": "the whole build: Engine::compute(coulomb, FockBuilder), full N^4",
+                                  "speedup_vs_reference_cpu": t / (ms * 1e-3),
+                                  "max_abs_dJ": float(np.max(np.abs(J.cpu().numpy() - Jr))),
+                                  "max_abs_dK": float(np.max(np.abs(K.cpu().numpy() - Kr)))}
+    out["cfg0_h2o8_sto3g"] = c0
+    del eng
+
+    # config 2: C12H26 / cc-pVTZ, plain FP64 and mixed (FP32 below Q_ij Q_kl max|D| = 1e-7)
+    w = lai.workloads.make("c12h26_ccpvtz")
+    eng = lai.Engine(w.basis, threshold=w.thr, device=dev.index)
+    D = torch.from_numpy(w.D).to(dev)
+    J, K = dev_mats(w.nbf)
+    J2, K2 = dev_mats(w.nbf)
+    ms64 = _device_ms(lambda: eng.jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr(), stream=s), flush, stream, steps)
+    rep = [None]
+
+    def mixed():
+        rep[0] = eng.jk_device(D.data_ptr(), J2.data_ptr(), K2.data_ptr(), stream=s, fp32_cut=MIXED_CUT)
+    ms32 = _device_ms(mixed, flush, stream, steps)
+    dE = float(0.5 * torch.sum(D * (J2 - J)).item() - 0.25 * torch.sum(D * (K2 - K)).item())
+    nq = eng.quartet_count()
+    out["cfg2_c12h26_ccpvtz"] = {
+        "system": SYSTEMS["c12h26_ccpvtz"], "nbf": w.nbf, "quartets": nq, "fp64_ms_per_build": ms64,
+        "fp64_quartets_per_s": nq / (ms64 * 1e-3), "mixed_ms_per_build": ms32, "fp32_cut": MIXED_CUT,
+        "mixed_speedup_vs_fp64": ms64 / ms32,
+        "fp32_fraction": rep[0].quartets_fp32 / max(1, rep[0].quartets_fp32 + rep[0].quartets_fp64),
+        "abs_dE": abs(dE), "max_abs_dJ": float(torch.max(torch.abs(J2 - J)).item()),
+        "max_abs_dK": float(torch.max(torch.abs(K2 - K)).item())}
+    del eng
+
+    # config 3: 256 clusters in one batched engine, every class one launch for all
+    # clusters, the build replayed as a CUDA graph; plain FP64 and mixed
+    cl = lai.workloads.clusters(256)
+    eng = lai.BatchedEngine([c.basis for c in cl], device=dev.index)
+    Dp = torch.from_numpy(eng.pack([c.D for c in cl])).to(dev)
+    Jp, Kp = torch.empty_like(Dp), torch.empty_like(Dp)
+    Jq, Kq = torch.empty_like(Dp), torch.empty_like(Dp)
+    reps = {}
+    gs = torch.cuda.Stream(device=dev)  # graph capture needs a stream other than the legacy default
+    torch.cuda.synchronize()
+
+    def batched(cut, Jo, Ko):
+        reps[cut] = eng.jk_device(Dp.data_ptr(), Jo.data_ptr(), Ko.data_ptr(), stream=gs.cuda_stream,
+                                  fp32_cut=cut, graph=True)
+    ms64 = _device_ms(lambda: batched(0.0, Jp, Kp), flush, gs, steps)
+    ms32 = _device_ms(lambda: batched(MIXED_CUT, Jq, Kq), flush, gs, steps)
+    off, _ = eng.layout()
+    Dh, dJ, dK = Dp.cpu().numpy(), (Jq - Jp).cpu().numpy(), (Kq - Kp).cpu().numpy()
+    dE = [0.5 * float(np.dot(Dh[a:b], dJ[a:b])) - 0.25 * float(np.dot(Dh[a:b], dK[a:b]))
+          for a, b in zip(off[:-1], off[1:])]
+    r = reps[MIXED_CUT]
+    nq = r.quartets_fp32 + r.quartets_fp64
+    out["cfg3_clusters256"] = {
+        "system": "256 water clusters, U{1..12} waters (seeded), cc-pVDZ", "quartets": int(nq),
+        "fp64_ms_per_build": ms64, "mixed_ms_per_build": ms32, "fp32_cut": MIXED_CUT,
+        "mixed_speedup_vs_fp64": ms64 / ms32, "mixed_quartets_per_s": nq / (ms32 * 1e-3),
+        "fp32_fraction": r.quartets_fp32 / max(1, nq), "per_cluster_max_abs_dE": float(np.max(np.abs(dE)))}
+    del eng
+
+    # config 4: (H2O)16 / cc-pVDZ nuclear gradient of E = tr(DJ)/2 - tr(DK)/4 (FP64)
+    w = lai.workloads.make("h2o16_ccpvdz")
+    eng = lai.Engine(w.basis, threshold=w.thr, device=dev.index)
+    D = torch.from_numpy(w.D).to(dev)
+    G = torch.empty((eng.natom(), 3), dtype=torch.float64, device=dev)
+    J, K = dev_mats(w.nbf)
+    lib = lai.lib()
+
+    def grad():
+        lai._lib.check(lib.lai_jk_gradient_device(eng._h, ctypes.c_void_p(D.data_ptr()),
+                                                  ctypes.c_void_p(G.data_ptr()), ctypes.c_void_p(s)))
+    msg = _device_ms(grad, flush, stream, 1)
+    msj = _device_ms(lambda: eng.jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr(), stream=s), flush, stream, steps)
+    out["cfg4_h2o16_gradient"] = {
+        "system": SYSTEMS["h2o16_ccpvdz"], "natom": int(G.shape[0]), "gradient_ms": msg, "jk_build_ms": msj,
+        "translational_invariance": float(torch.max(torch.abs(G.sum(dim=0))).item())}
+    return out
 
 def main():
     args = parse()
@@ -615,6 +767,13 @@ def main():
             mixed = mixed_leg(eng, D, J, K, flush, stream, args.steps, ms_per_step)
         except Exception as ex:  # report, do not lose the FP64 line
             mixed = {"error": f"{type(ex).__name__}: {ex}"}
+    configs = None
+    if ws == 1 and not args.no_configs and args.workload == WORKLOAD:
+        try:
+            configs = side_configs(lai, dev, flush, stream, min(args.steps, 2),
+                                   cpu_baseline=not args.no_cpu_baseline)
+        except Exception as ex:  # report, do not lose the headline line
+            configs = {"error": f"{type(ex).__name__}: {ex}"}
     pms, pfl, pfx, pcl = pr["ms"], pr["alg_flops"], pr["alg_flops_executed"], pr["lclass"]
     peak = lai.probe_fp64_peak(local)
     roof_all = float(np.sum(pfx) / (np.sum(pms) * 1e-3) / 1e12)
@@ -682,6 +841,7 @@ def main():
             "setup_s": setup_s,
             "autotune": tune,
             "mixed": mixed,
+            "configs": configs,
         }
         if cpu:
             out["cpu_baseline"] = cpu
