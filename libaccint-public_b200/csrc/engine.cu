@@ -292,6 +292,22 @@ int upload_class(PairClassHost& c) {
   LAI_CUDA_TRY(upload(c.d_prim, c.prim));
   if (c.Q.empty()) c.Q.assign(c.n(), 0.0);
   LAI_CUDA_TRY(upload(c.d_Q, c.Q));
+  {  // per-pair primitive records (lai::BraRecField), FP64 and FP32
+    const int n = c.n(), Kab = c.Ka * c.Kb;
+    std::vector<double> rb((size_t)n * Kab * lai::kBraRec, 0.0);
+    static const int from[lai::kBraRec] = {lai::PF_Q,  lai::PF_ZETA, lai::PF_HZ,  lai::PF_C,
+                                           lai::PF_PX, lai::PF_PY,   lai::PF_PZ,  -1,
+                                           lai::PF_PAX, lai::PF_PAY, lai::PF_PAZ, -1};
+    for (int p = 0; p < n; ++p)
+      for (int t = 0; t < Kab; ++t)
+        for (int f = 0; f < lai::kBraRec; ++f)
+          if (from[f] >= 0)
+            rb[((size_t)p * Kab + t) * lai::kBraRec + f] = c.prim[((size_t)from[f] * Kab + t) * n + p];
+    std::vector<float> rbf(rb.size());
+    for (size_t i = 0; i < rb.size(); ++i) rbf[i] = (float)rb[i];
+    LAI_CUDA_TRY(upload(c.d_primb, rb));
+    LAI_CUDA_TRY(upload(c.d_primbf, rbf));
+  }
   return LAI_OK;
 }
 

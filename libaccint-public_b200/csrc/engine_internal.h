@@ -87,7 +87,7 @@ struct PairClassHost {
   std::vector<double> prim;        // SoA [PF_COUNT][Kab][n]
   int n() const { return (int)sa.size(); }
   // device copies
-  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_Acen, d_prim, d_sys, d_primf;
+  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_Acen, d_prim, d_sys, d_primf, d_primb, d_primbf;
   bool batched = false;             // d_sys is set (more than one system)
   lai::PairClassDev view() const {
     lai::PairClassDev v;
@@ -99,6 +99,8 @@ struct PairClassHost {
     v.qprim_max = qprim_max;
     v.sys = batched ? d_sys.as<int>() : nullptr;
     v.primf = d_primf.as<float>();
+    v.primb = d_primb.as<double>();
+    v.primbf = d_primbf.as<float>();
     return v;
   }
 };

@@ -153,6 +153,14 @@ __device__ __forceinline__ const double* prim_table<double>(const PairClassDev& 
 template <>
 __device__ __forceinline__ const float* prim_table<float>(const PairClassDev& c) { return c.primf; }
 
+// Per-pair primitive records (BraRecField) in the kernel's compute type.
+template <typename R>
+__device__ __forceinline__ const R* bra_records(const PairClassDev& c);
+template <>
+__device__ __forceinline__ const double* bra_records<double>(const PairClassDev& c) { return c.primb; }
+template <>
+__device__ __forceinline__ const float* bra_records<float>(const PairClassDev& c) { return c.primbf; }
+
 // Bra primitive-pair data of one pair (same fields, bra side).
 struct BraPrim {
   double q, zeta, hz, px, py, pz, pax, pay, paz, c;

@@ -29,6 +29,28 @@
 #include "eri_tables_smem.cuh"
 #include "fp32_tables.h"
 
+#ifndef LAI_KET_OUTER_ALL
+#define LAI_KET_OUTER_ALL 0
+#endif
+#ifndef LAI_FOLD_RELOAD
+#define LAI_FOLD_RELOAD 0
+#endif
+#ifndef LAI_MINB_L1
+#define LAI_MINB_L1 3
+#endif
+#ifndef LAI_MINB_L0
+#define LAI_MINB_L0 4
+#endif
+#ifndef LAI_K0_REG
+#define LAI_K0_REG 0
+#endif
+#ifndef LAI_MINB_F32_L1
+#define LAI_MINB_F32_L1 4
+#endif
+#ifndef LAI_PREFETCH_D
+#define LAI_PREFETCH_D 0
+#endif
+
 namespace lai {
 
 namespace {
@@ -111,7 +133,7 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   // bra and ket pairs' first centres, formed in FP64, so that the error of P - Q
   // scales with |P - A| rather than with the absolute coordinates.  FP64: P - Q
   // from the stored centres P and Q (no extra registers held across the loop).
-  R AC[3];
+  R AC[3] = {R(0), R(0), R(0)};
   if constexpr (F32) {
 #pragma unroll
     for (int x = 0; x < 3; ++x)
@@ -130,7 +152,27 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   struct BraVals {
     R zeta, hz, Px, Py, Pz, PAx, PAy, PAz, cab;
   };
+  const R* __restrict__ bprimb = bra_records<R>(blk.bra);
   auto load_bra = [&](int ib, R& qab, BraVals& v) {
+    if (uniform_bra || SPLIT) {
+      // the warp (or the lane group) reads one pair's primitives: its contiguous
+      // per-pair records, 16-byte vector loads
+      const R* rb = bprimb + ((size_t)p * Kab + ib) * kBraRec;
+      if constexpr (F32) {
+        const float4* r4 = reinterpret_cast<const float4*>(rb);
+        const float4 a = __ldg(r4), c = __ldg(r4 + 2);
+        qab = a.x; v.zeta = a.y; v.hz = a.z; v.cab = a.w;
+        v.PAx = c.x; v.PAy = c.y; v.PAz = c.z;
+      } else {
+        const double2* r2 = reinterpret_cast<const double2*>(rb);
+        const double2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2), d = __ldg(r2 + 3),
+                      e = __ldg(r2 + 4), f = __ldg(r2 + 5);
+        qab = a.x; v.zeta = a.y; v.hz = b.x; v.cab = b.y;
+        v.Px = c.x; v.Py = c.y; v.Pz = d.x;
+        v.PAx = e.x; v.PAy = e.y; v.PAz = f.x;
+      }
+      return;
+    }
     const R* pb = bprim + (size_t)ib * nbra + p;
     qab = __ldg(pb + PF_Q * sb);
     v.zeta = __ldg(pb + PF_ZETA * sb);
@@ -144,6 +186,39 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
     v.PAy = __ldg(pb + PF_PAY * sb);
     v.PAz = __ldg(pb + PF_PAZ * sb);
     v.cab = __ldg(pb + PF_C * sb);
+  };
+  // One-root classes accumulate per row of the inner primitive loop: the factor
+  // constant along the row (the outer pair's contraction coefficient; for (ps|ss)
+  // also PA) multiplies the row sums once, when the row ends (fold_row):
+  //   (ss|ss): S0 = sum c' rs F_0;  (ps|ss): S0 as above, S1_i = sum PQ_i c' rs rz F_1,
+  //   G_i += c (PA_i S0 - S1_i),
+  // with c' the inner pair's coefficient.
+  constexpr bool kKetOuter = LAI_KET_OUTER_ALL ? true : (LAB == LCD);
+  constexpr bool kFold = NR == 1 && (LAB == 0 || !kKetOuter);
+  R S0 = R(0), S1[3] = {R(0), R(0), R(0)};
+  auto fold_row = [&](R rowc, const BraVals& bv, int ib) {
+    if constexpr (kFold) {
+      if constexpr (LAB == 0) {
+        G[0] += rowc * S0;
+      } else {
+        R PA[3] = {bv.PAx, bv.PAy, bv.PAz};
+        if constexpr (LAI_FOLD_RELOAD) {
+          const R* pb = bprim + (size_t)ib * nbra + p;
+          PA[0] = __ldg(pb + PF_PAX * sb);
+          PA[1] = __ldg(pb + PF_PAY * sb);
+          PA[2] = __ldg(pb + PF_PAZ * sb);
+          rowc = __ldg(pb + PF_C * sb);
+        }
+        sfor<0, NE>([&](auto IE) {
+          constexpr int ie = decltype(IE)::value;
+          constexpr int ce = cart_comp(LA, ie);
+          constexpr int d = comp_x(ce) ? 0 : comp_y(ce) ? 1 : 2;
+          G[ie] += rowc * (PA[d] * S0 - S1[d]);
+        });
+        S1[0] = S1[1] = S1[2] = R(0);
+      }
+      S0 = R(0);
+    }
   };
   auto prim = [&](const BraVals& bv, const KetPrimT<R>& cur) {
     const R zeta = bv.zeta, hz = bv.hz, cab = bv.cab;
@@ -160,29 +235,33 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
     const R inv = rs * rs;
     const R rz = eta * inv, re = zeta * inv;
     const R T = zeta * rz * (PQx * PQx + PQy * PQy + PQz * PQz);
-    const R pref = cab * ccd * rs;
     if constexpr (NR == 1) {
       // One root: (ss|ss) = pref F_0 and (p_i s|ss) = pref (PA_i F_0 - rz PQ_i F_1)
       // -- the one-point Rys rule (w = F_0, u = F_1/F_0) written without its
-      // quotient.
+      // quotient -- summed per row (fold_row) without the row's constant factor.
       R F0, F1;
       if constexpr (F32) boys01_f32(T, stab, F0, F1); else boys01_smem<R>(T, stab, F0, F1);
-      const R pw0 = pref * F0;
-      if constexpr (LAB == 0) {
-        G[0] += pw0;
+      static_assert(LAB == 0 || (LA == 1 && LB == 0 && LCD == 0), "one-root classes: (ss|ss), (ps|ss)");
+      if constexpr (kFold) {
+        const R pv = (kKetOuter ? cab : ccd) * rs;
+        S0 += pv * F0;
+        if constexpr (LAB == 1) {
+          const R pw1 = pv * rz * F1;
+          S1[0] += PQx * pw1;
+          S1[1] += PQy * pw1;
+          S1[2] += PQz * pw1;
+        }
       } else {
-        static_assert(LA == 1 && LB == 0 && LCD == 0, "one-root classes: (ss|ss), (ps|ss)");
-        const R pw1 = pref * rz * F1;
-        const R PA[3] = {PAx, PAy, PAz}, PQ[3] = {PQx, PQy, PQz};
-        sfor<0, NE>([&](auto IE) {
-          constexpr int ie = decltype(IE)::value;
-          constexpr int ce = cart_comp(LA, ie);
-          constexpr int d = comp_x(ce) ? 0 : comp_y(ce) ? 1 : 2;
-          G[ie] += PA[d] * pw0 - PQ[d] * pw1;
-        });
+        // (ps|ss) with the ket loop outside: PA changes along the inner loop
+        const R pref = cab * ccd * rs;
+        const R pw0 = pref * F0, pw1 = pref * rz * F1;
+        G[0] += PAx * pw0 - PQx * pw1;
+        G[1] += PAy * pw0 - PQy * pw1;
+        G[2] += PAz * pw0 - PQz * pw1;
       }
       return;
     }
+    const R pref = cab * ccd * rs;
     R u[NR], w[NR];
     if constexpr (F32) rys_f32(NR, T, stab, tab.herm_x2, tab.herm_w, u, w);
     else rys_smem<NR, R>(T, stab, tab, u, w);
@@ -234,9 +313,30 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   // 32 ket rows no longer fit in L1).  Otherwise the ket side usually has more
   // primitives (s pairs against p/d pairs) and goes inside, with its next primitive
   // pair loaded one iteration ahead.
-  constexpr bool kKetOuter = (LAB == LCD);
   const R* pk0 = kprim + q;
   const R peps_r = R(peps);
+  if constexpr (LAI_PREFETCH_D) {
+    // the density lines the digestion reads (per lane: the (c, d), (b, d), (b, c),
+    // (a, d), (a, c) blocks), requested into L1 now, read after the primitive loop
+    if (args.mode == MODE_JK && !blk.bra.sys) {
+      const int fa = __ldg(blk.bra.func_a + p), fb = __ldg(blk.bra.func_b + p);
+      const int fc = __ldg(blk.ket.func_a + q), fd = __ldg(blk.ket.func_b + q);
+      const double* D = args.D;
+      const size_t n = (size_t)args.nbf;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) prefetch_l1(D + (fc + c) * n + fd);
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        prefetch_l1(D + (fb + b) * n + fd);
+        prefetch_l1(D + (fb + b) * n + fc);
+      }
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        prefetch_l1(D + (fa + a) * n + fd);
+        prefetch_l1(D + (fa + a) * n + fc);
+      }
+    }
+  }
   if constexpr (kKetOuter) {
     const R qab_max = ib0 < Kab ? __ldg(bprim + (size_t)ib0 * nbra + p + PF_Q * sb) : R(0);
     KetPrimT<R> nxt;
@@ -245,25 +345,28 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
       const KetPrimT<R> cur = nxt;
       if (qab_max * cur.q < peps_r || ib0 >= Kab) break;
       if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
+      BraVals bv{};
       for (int ib = ib0; ib < Kab; ib += ibs) {
         R qab;
-        BraVals bv;
         load_bra(ib, qab, bv);
         if (qab * cur.q < peps_r) break;
         ++nprim_done;
         prim(bv, cur);
       }
+      fold_row(R(cur.c), bv, 0);
       merge();
     }
   } else {
     const R qket_max = R(blk.ket.qprim_max);
+    KetPrimT<R> k0;
+    if constexpr (LAI_K0_REG) load_ket_prim(pk0, sk, k0);  // the first ket primitive opens every row
     for (int ib = ib0; ib < Kab; ib += ibs) {
       R qab;
       BraVals bv;
       load_bra(ib, qab, bv);
       if (qab * qket_max < peps_r) break;
       KetPrimT<R> nxt;
-      load_ket_prim(pk0, sk, nxt);
+      if constexpr (LAI_K0_REG) nxt = k0; else load_ket_prim(pk0, sk, nxt);
       for (int ik = 0; ik < Kcd; ++ik) {
         const KetPrimT<R> cur = nxt;
         if (qab * cur.q < peps_r) break;
@@ -271,6 +374,7 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
         ++nprim_done;
         prim(bv, cur);
       }
+      fold_row(bv.cab, bv, ib);
       merge();
     }
   }
@@ -548,7 +652,7 @@ __device__ __forceinline__ void small_finish(GV&& gval, const QuartetBlock& blk,
 template <int LA, int LB, int LC, int LD, typename R>
 __host__ __device__ constexpr int small_min_blocks() {
   constexpr int L = LA + LB + LC + LD;
-  return sizeof(R) == 8 ? (L == 0 ? 4 : L == 1 ? 3 : 0) : (L <= 1 ? 4 : L == 2 ? 2 : 0);
+  return sizeof(R) == 8 ? (L == 0 ? LAI_MINB_L0 : L == 1 ? LAI_MINB_L1 : 0) : (L <= 1 ? LAI_MINB_F32_L1 : L == 2 ? 2 : 0);
 }
 
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>

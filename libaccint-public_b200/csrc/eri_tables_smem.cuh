@@ -16,16 +16,35 @@ namespace lai {
 
 // Shared-memory table layouts, in elements of the compute type R (the FP32 kernels
 // stage FP32 copies: half the shared memory, and single-width loads).
-constexpr int kBoysRow = 10;   // FP64: F_0..F_9 per grid point, five 16-byte units (odd)
-constexpr int kBoysRowF = 12;  // FP32: F_0..F_11, three 16-byte units (odd)
+//
+// FP64 Boys rows hold the Taylor coefficients already divided by j!: c_j =
+// F_j(T0)/j! and d_j = F_{j+1}(T0)/j!, j < 8, so that F_0(T0 - x) = sum c_j x^j
+// and F_1(T0 - x) = sum d_j x^j are plain Horner chains (no x/j products per
+// quartet); 16 values and two pad doubles (nine 16-byte units, odd, so lanes on
+// different rows spread over the banks).  The grid stops at T0 = 38.3
+// (kBoysRowsS rows); from T = 38.3 on the asymptotic forms are used, whose
+// relative error there is below 2e-16 for F_0 and F_1 (e^-T / (2T) against
+// F_1 ~ sqrt(pi/T) / (4T)).
+#ifndef LAI_BOYS_PREDIV
+#define LAI_BOYS_PREDIV 0
+#endif
+constexpr int kBoysRowsS = LAI_BOYS_PREDIV ? 384 : kBoysNGrid;   // FP64 rows staged, T0 = k / 10
+constexpr double kBoysTmaxS = LAI_BOYS_PREDIV ? 38.3 : kBoysTmax;
+constexpr int kBoysRowS = LAI_BOYS_PREDIV ? 18 : 10;     // c_0..c_7, d_0..d_7, 2 pad | F_0..F_9
+constexpr int kBoysRowF = 12;     // FP32: F_0..F_11, three 16-byte units (odd)
 template <typename R>
-__host__ __device__ constexpr int boys_row() { return sizeof(R) == 8 ? kBoysRow : kBoysRowF; }
+__host__ __device__ constexpr int boys_row() { return sizeof(R) == 8 ? kBoysRowS : kBoysRowF; }
+template <typename R>
+__host__ __device__ constexpr int boys_rows() { return sizeof(R) == 8 ? kBoysRowsS : kBoysNGrid; }
 template <int NR>
 __host__ __device__ constexpr int rys_row() { return 24 * NR + 2; }  // 12 degrees x NR x (u,w) + pad
 template <int NR, typename R>
 __host__ __device__ constexpr int table_elems() {
-  return NR == 1 ? kBoysNGrid * boys_row<R>() : rys_tmax_c(NR) * rys_row<NR>();
+  return NR == 1 ? boys_rows<R>() * boys_row<R>() : rys_tmax_c(NR) * rys_row<NR>();
 }
+// 1.5 * 2^52: adding it to a double y with 0 <= |y| < 2^31 leaves rint(y) in the
+// low word of the sum (round to nearest even), with no conversion instruction.
+constexpr double kRoundMagicD = 6755399441055744.0;
 template <int NR, typename R>
 __host__ __device__ constexpr size_t table_bytes() {
   return (sizeof(R) * table_elems<NR, R>() + 15) & ~size_t(15);  // what follows stays 16-byte aligned
@@ -33,7 +52,26 @@ __host__ __device__ constexpr size_t table_bytes() {
 
 template <int NR, typename R>
 __device__ __forceinline__ void stage_table(R* __restrict__ st, const RysTablesView& tab) {
-  if constexpr (NR == 1) {
+  if constexpr (NR == 1 && sizeof(R) == 8 && !LAI_BOYS_PREDIV) {
+    constexpr int NV = kBoysRowS;
+    for (int i = threadIdx.x; i < kBoysRowsS * NV; i += blockDim.x) {
+      const int k = i / NV, j = i - k * NV;
+      st[k * NV + j] = __ldg(tab.boys + k * kBoysNM + j);
+    }
+  } else if constexpr (NR == 1 && sizeof(R) == 8) {
+    constexpr int NV = kBoysRowS;
+    for (int i = threadIdx.x; i < kBoysRowsS * NV; i += blockDim.x) {
+      const int k = i / NV, j = i - k * NV;
+      // j < 8: c_j = F_j / j!; 8 <= j < 16: d_{j-8} = F_{j-7} / (j-8)!; then pad
+      const int m = j < 8 ? j : j - 8;
+      double f = 0.0;
+      if (j < 16) {
+        f = __ldg(tab.boys + k * kBoysNM + (j < 8 ? j : j - 7));
+        for (int q = 2; q <= m; ++q) f /= q;
+      }
+      st[k * NV + j] = R(f);
+    }
+  } else if constexpr (NR == 1) {
     constexpr int NV = boys_row<R>();  // values per row (the row holds no padding)
     for (int i = threadIdx.x; i < kBoysNGrid * NV; i += blockDim.x) {
       const int k = i / NV, j = i - k * NV;
@@ -49,28 +87,56 @@ __device__ __forceinline__ void stage_table(R* __restrict__ st, const RysTablesV
   }
 }
 
-// F_0(T) and F_1(T) from the staged Boys grid (same arithmetic as boys01 in
-// rys_eval.h).
+// F_0(T) and F_1(T) from the staged Boys grid (the Taylor series of boys01 in
+// rys_eval.h; FP64 from the pre-divided rows).
 template <typename R>
 __device__ __forceinline__ void boys01_smem(R T, const R* __restrict__ st, R& F0, R& F1) {
   constexpr bool F64 = sizeof(R) == 8;
-  if (T < R(kBoysTmax)) {
-    // nearest grid point; in FP32, T just below kBoysTmax can round up to the
-    // row past the end, hence the clamp
-    const int k = min(F64 ? __double2int_rn(double(T) * 10.0) : __float2int_rn(float(T) * 10.0f),
-                      kBoysNGrid - 1);
-    const R x = R(k) * R(0.1) - T;
-    constexpr int NG = boys_terms<R>() + 1;  // grid values used: F_0..F_N
-    R g[12];
-    if constexpr (F64) {
-      const double2* f = reinterpret_cast<const double2*>(st + k * kBoysRow);
+  if constexpr (F64) {
+    // FP64: nearest grid point by the rounding constant, Horner on the pre-divided
+    // rows (8 terms each; the first omitted term is below 6e-17 relative)
+    if (T < kBoysTmaxS) {
+      const double km = fma(double(T), 10.0, kRoundMagicD);
+      const int k = min(__double2loint(km), kBoysRowsS - 1);
+      const double x = fma(km - kRoundMagicD, 0.1, -double(T));
+      const double2* f = reinterpret_cast<const double2*>(st + k * kBoysRowS);
+      if constexpr (LAI_BOYS_PREDIV) {
+        const double2 c67 = f[3], d67 = f[7];
+        double a = fma(c67.y, x, c67.x), b = fma(d67.y, x, d67.x);
 #pragma unroll
-      for (int j = 0; j < (NG + 1) / 2; ++j) {
-        const double2 v = f[j];
-        g[2 * j] = v.x;
-        g[2 * j + 1] = v.y;
+        for (int j = 2; j >= 0; --j) {
+          const double2 c = f[j], d = f[4 + j];
+          a = fma(fma(a, x, c.y), x, c.x);
+          b = fma(fma(b, x, d.y), x, d.x);
+        }
+        F0 = R(a);
+        F1 = R(b);
+      } else {
+        double g[10];
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+          const double2 v = f[j];
+          g[2 * j] = v.x;
+          g[2 * j + 1] = v.y;
+        }
+        double a, b;
+        boys_taylor<double>(x, g, a, b);
+        F0 = R(a);
+        F1 = R(b);
       }
     } else {
+      const R rt = fast_rsqrt(T);
+      F0 = R(0.88622692545275801365) * rt;  // sqrt(pi)/2
+      F1 = R(0.5) * F0 * rt * rt;
+    }
+  } else {
+    // FP32: nearest grid point; T just below kBoysTmax can round up to the row past
+    // the end, hence the clamp
+    if (T < R(kBoysTmax)) {
+      const int k = min(__float2int_rn(float(T) * 10.0f), kBoysNGrid - 1);
+      const R x = R(k) * R(0.1) - T;
+      constexpr int NG = boys_terms<R>() + 1;  // grid values used: F_0..F_N
+      R g[12];
       const float4* f = reinterpret_cast<const float4*>(st + k * kBoysRowF);
 #pragma unroll
       for (int j = 0; j < (NG + 3) / 4; ++j) {
@@ -80,12 +146,12 @@ __device__ __forceinline__ void boys01_smem(R T, const R* __restrict__ st, R& F0
         g[4 * j + 2] = v.z;
         g[4 * j + 3] = v.w;
       }
+      boys_taylor<R>(x, g, F0, F1);
+    } else {
+      const R rt = fast_rsqrt(T);
+      F0 = R(0.88622692545275801365) * rt;  // sqrt(pi)/2
+      F1 = R(0.5) * F0 * rt * rt;
     }
-    boys_taylor<R>(x, g, F0, F1);
-  } else {
-    const R rt = fast_rsqrt(T);
-    F0 = R(0.88622692545275801365) * rt;  // sqrt(pi)/2
-    F1 = R(0.5) * F0 * rt * rt;
   }
 }
 
@@ -106,8 +172,18 @@ __device__ __forceinline__ void rys_smem(R T, const R* __restrict__ st, const Ry
     }
   } else {
     if (T < R(rys_tmax_c(NR))) {
-      const int k = (int)T;
-      const R x = R(2) * (T - R(k)) - R(1);
+      int k;
+      R x;
+      if constexpr (F64) {
+        // unit interval by the rounding constant: rint(T - 1/2) (an integer T may
+        // land on the interval below, at its end x = 1)
+        const double km = (double(T) - 0.5) + kRoundMagicD;
+        k = __double2loint(km);
+        x = fma(2.0, double(T) - (km - kRoundMagicD), -1.0);
+      } else {
+        k = (int)T;
+        x = R(2) * (T - R(k)) - R(1);
+      }
       using V2 = typename std::conditional<F64, double2, float2>::type;
       const V2* c = reinterpret_cast<const V2*>(st + k * rys_row<NR>());
 #pragma unroll

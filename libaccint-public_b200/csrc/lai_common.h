@@ -41,6 +41,18 @@ enum PrimField : int {
   PF_COUNT
 };
 
+// The same primitive-pair data per pair (AoS), for the kernels whose whole warp
+// reads one pair's primitives (the bra of the thread-per-quartet kernels): record
+// [p][t][kBraRec] with the fields below, so that one pair's primitives are a few
+// contiguous cache lines (SoA by pair index spreads them over one line per field
+// and primitive) and each record is read with 16-byte vector loads.
+enum BraRecField : int {
+  BR_Q = 0, BR_ZETA, BR_HZ, BR_C,   // first 16 bytes (FP32) / first two double2 (FP64)
+  BR_PX, BR_PY, BR_PZ, BR_PAD0,
+  BR_PAX, BR_PAY, BR_PAZ, BR_PAD1,
+  kBraRec
+};
+
 struct PairClassDev {
   int la, lb;          // la >= lb (pairs are oriented so the bra-side HRR moves to the smaller l)
   int Ka, Kb;          // nonzero primitive counts
@@ -56,6 +68,8 @@ struct PairClassDev {
   double qprim_max;    // largest PF_Q of the class
   const int* sys;      // [npairs] system of each pair in a batched engine, else nullptr
   const float* primf;  // FP32 copy of prim (the FP32 kernels of mixed precision)
+  const double* primb;  // [npairs][Ka*Kb][kBraRec] per-pair records (BraRecField)
+  const float* primbf;  // FP32 copy of primb
 };
 
 // One launch: the canonical quartets (p, q) with p a pair of class `bra` and q a
