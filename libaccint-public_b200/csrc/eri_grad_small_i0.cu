@@ -1,0 +1,15 @@
+// Explicit instantiations of the thread-per-quartet gradient kernels (part 1
+// of 3; split so nvcc compiles the classes in parallel).
+#include "eri_grad_small.cuh"
+
+namespace lai {
+namespace grad_small {
+
+#define X(a, b, c, d)                                                                                \
+  template int launch<a, b, c, d>(const QuartetBlock&, const GradSmallArgs&, const RysTablesView&, \
+                                  cudaStream_t, int);
+X(0, 0, 0, 0) X(1, 0, 0, 0) X(1, 0, 1, 0) X(1, 1, 0, 0)
+#undef X
+
+}  // namespace grad_small
+}  // namespace lai

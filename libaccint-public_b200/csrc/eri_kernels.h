@@ -57,5 +57,10 @@ int launch_grad(const QuartetBlock& blk, const double* D, int nbf, const int* sh
                 double prim_eps, const RysTablesView& tab, cudaStream_t stream, double* gscratch,
                 size_t gscratch_doubles, int num_sms);
 size_t grad_global_scratch_doubles(int la, int lb, int lc, int ld, int num_sms);
+// Thread-per-quartet gradient kernels for the low classes (eri_grad_small.cu): 0 when
+// launched, -1 when the class is not covered (use launch_grad), -3 on a CUDA error.
+int launch_grad_small(const QuartetBlock& blk, const double* D, int nbf, const int* shell_atom, double* grad,
+                      double prim_eps, const RysTablesView& tab, cudaStream_t stream, int num_sms);
+bool grad_small_supported(int la, int lb, int lc, int ld);
 
 }  // namespace lai

@@ -51,6 +51,11 @@ int lai_jk_gradient_device(lai_engine* engine, const double* d_D, double* d_grad
   const int nbf = (int)engine->basis->nbf;
   for (const auto& bp : engine->blocks) {
     const lai::QuartetBlock q = make_block(engine, *bp);
+    const int rs = lai::launch_grad_small(q, d_D, nbf, engine->d_shell_atom.as<int>(), d_grad, engine->prim_eps,
+                                          engine->tab, s, engine->num_sms);
+    if (rs == 0) continue;
+    if (rs != -1)
+      return fail(LAI_ECUDA, std::string("gradient launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     const size_t need = lai::grad_global_scratch_doubles(q.bra.la, q.bra.lb, q.ket.la, q.ket.lb,
                                                          engine->num_sms);
     if (int rc = ensure_scratch(engine, need)) return rc;
