@@ -61,7 +61,8 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 
   const int Kab = blk.bra.Ka * blk.bra.Kb;
   const int Kcd = blk.ket.Ka * blk.ket.Kb;
-  const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
+  const size_t sk = (size_t)Kcd * nket;
+  (void)nbra;
 
   R G[NK * NF];
 #pragma unroll
@@ -70,18 +71,21 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
   const double peps = args.prim_eps;
   unsigned int nprim_done = 0;
   for (int ib = 0; ib < Kab; ++ib) {
-    const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
+    // the bra pair's primitive record (BraRecField): the lanes of a quartet group
+    // (and usually the whole warp) read the same contiguous record
+    const double2* rb = reinterpret_cast<const double2*>(blk.bra.primb + ((size_t)p * Kab + ib) * kBraRec);
+    const double2 b0 = __ldg(rb), b1 = __ldg(rb + 1);
     // primitive pairs are sorted by their Schwarz bound: once the bra bound times
     // the largest ket bound of the class drops below the cut, the rest do too
-    const double qab = __ldg(pb + PF_Q * sb);
+    const double qab = b0.x;
     if (qab * blk.ket.qprim_max < peps) break;
-    const R zeta = R(__ldg(pb + PF_ZETA * sb));
-    const R hz = R(__ldg(pb + PF_HZ * sb));
+    const double2 b2 = __ldg(rb + 2), b3 = __ldg(rb + 3), b4 = __ldg(rb + 4), b5 = __ldg(rb + 5);
+    const R zeta = R(b0.y);
+    const R hz = R(b1.x);
     // P - Q in FP64 on both paths (centres are O(10) bohr)
-    const double Px = __ldg(pb + PF_PX * sb), Py = __ldg(pb + PF_PY * sb), Pz = __ldg(pb + PF_PZ * sb);
-    const R PAx = R(__ldg(pb + PF_PAX * sb)), PAy = R(__ldg(pb + PF_PAY * sb)),
-            PAz = R(__ldg(pb + PF_PAZ * sb));
-    const R cab = R(__ldg(pb + PF_C * sb));
+    const double Px = b2.x, Py = b2.y, Pz = b3.x;
+    const R PAx = R(b4.x), PAy = R(b4.y), PAz = R(b5.x);
+    const R cab = R(b1.y);
     const double* pk0 = blk.ket.prim + q;
     KetPrim nxt;
     load_ket_prim(pk0, sk, nxt);

@@ -29,28 +29,6 @@
 #include "eri_tables_smem.cuh"
 #include "fp32_tables.h"
 
-#ifndef LAI_KET_OUTER_ALL
-#define LAI_KET_OUTER_ALL 0
-#endif
-#ifndef LAI_FOLD_RELOAD
-#define LAI_FOLD_RELOAD 0
-#endif
-#ifndef LAI_MINB_L1
-#define LAI_MINB_L1 3
-#endif
-#ifndef LAI_MINB_L0
-#define LAI_MINB_L0 4
-#endif
-#ifndef LAI_K0_REG
-#define LAI_K0_REG 0
-#endif
-#ifndef LAI_MINB_F32_L1
-#define LAI_MINB_F32_L1 4
-#endif
-#ifndef LAI_PREFETCH_D
-#define LAI_PREFETCH_D 0
-#endif
-
 namespace lai {
 
 namespace {
@@ -193,22 +171,15 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   //   (ss|ss): S0 = sum c' rs F_0;  (ps|ss): S0 as above, S1_i = sum PQ_i c' rs rz F_1,
   //   G_i += c (PA_i S0 - S1_i),
   // with c' the inner pair's coefficient.
-  constexpr bool kKetOuter = LAI_KET_OUTER_ALL ? true : (LAB == LCD);
+  constexpr bool kKetOuter = (LAB == LCD);
   constexpr bool kFold = NR == 1 && (LAB == 0 || !kKetOuter);
   R S0 = R(0), S1[3] = {R(0), R(0), R(0)};
-  auto fold_row = [&](R rowc, const BraVals& bv, int ib) {
+  auto fold_row = [&](R rowc, const BraVals& bv) {
     if constexpr (kFold) {
       if constexpr (LAB == 0) {
         G[0] += rowc * S0;
       } else {
-        R PA[3] = {bv.PAx, bv.PAy, bv.PAz};
-        if constexpr (LAI_FOLD_RELOAD) {
-          const R* pb = bprim + (size_t)ib * nbra + p;
-          PA[0] = __ldg(pb + PF_PAX * sb);
-          PA[1] = __ldg(pb + PF_PAY * sb);
-          PA[2] = __ldg(pb + PF_PAZ * sb);
-          rowc = __ldg(pb + PF_C * sb);
-        }
+        const R PA[3] = {bv.PAx, bv.PAy, bv.PAz};
         sfor<0, NE>([&](auto IE) {
           constexpr int ie = decltype(IE)::value;
           constexpr int ce = cart_comp(LA, ie);
@@ -315,28 +286,6 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   // pair loaded one iteration ahead.
   const R* pk0 = kprim + q;
   const R peps_r = R(peps);
-  if constexpr (LAI_PREFETCH_D) {
-    // the density lines the digestion reads (per lane: the (c, d), (b, d), (b, c),
-    // (a, d), (a, c) blocks), requested into L1 now, read after the primitive loop
-    if (args.mode == MODE_JK && !blk.bra.sys) {
-      const int fa = __ldg(blk.bra.func_a + p), fb = __ldg(blk.bra.func_b + p);
-      const int fc = __ldg(blk.ket.func_a + q), fd = __ldg(blk.ket.func_b + q);
-      const double* D = args.D;
-      const size_t n = (size_t)args.nbf;
-#pragma unroll
-      for (int c = 0; c < NC; ++c) prefetch_l1(D + (fc + c) * n + fd);
-#pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        prefetch_l1(D + (fb + b) * n + fd);
-        prefetch_l1(D + (fb + b) * n + fc);
-      }
-#pragma unroll
-      for (int a = 0; a < NA; ++a) {
-        prefetch_l1(D + (fa + a) * n + fd);
-        prefetch_l1(D + (fa + a) * n + fc);
-      }
-    }
-  }
   if constexpr (kKetOuter) {
     const R qab_max = ib0 < Kab ? __ldg(bprim + (size_t)ib0 * nbra + p + PF_Q * sb) : R(0);
     KetPrimT<R> nxt;
@@ -353,20 +302,21 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
         ++nprim_done;
         prim(bv, cur);
       }
-      fold_row(R(cur.c), bv, 0);
+      fold_row(R(cur.c), bv);
       merge();
     }
   } else {
     const R qket_max = R(blk.ket.qprim_max);
+    // the first ket primitive opens every row: loaded once per quartet
     KetPrimT<R> k0;
-    if constexpr (LAI_K0_REG) load_ket_prim(pk0, sk, k0);  // the first ket primitive opens every row
+    load_ket_prim(pk0, sk, k0);
     for (int ib = ib0; ib < Kab; ib += ibs) {
       R qab;
       BraVals bv;
       load_bra(ib, qab, bv);
       if (qab * qket_max < peps_r) break;
       KetPrimT<R> nxt;
-      if constexpr (LAI_K0_REG) nxt = k0; else load_ket_prim(pk0, sk, nxt);
+      nxt = k0;
       for (int ik = 0; ik < Kcd; ++ik) {
         const KetPrimT<R> cur = nxt;
         if (qab * cur.q < peps_r) break;
@@ -374,7 +324,7 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
         ++nprim_done;
         prim(bv, cur);
       }
-      fold_row(bv.cab, bv, ib);
+      fold_row(bv.cab, bv);
       merge();
     }
   }
@@ -646,13 +596,16 @@ __device__ __forceinline__ void small_finish(GV&& gval, const QuartetBlock& blk,
 // Blocks per SM the register allocation must allow (ptxas caps registers at
 // 65536 / (256 * blocks)).  The light classes are latency bound with short
 // dependent chains and need the warps: in FP64 (ss|ss) fits 64 registers (4
-// blocks, 32 warps) and (ps|ss) 80 (3 blocks); in FP32 the one-root classes fit 64
-// and the L = 2 ones, with their compensated accumulators, 128 (2 blocks).  The other classes keep ptxas's own choice (0 = no bound;
-// an explicit 1 would let it take up to 255 registers).
+// blocks, 32 warps); (ps|ss), with the first ket primitive held across its bra
+// rows, takes up to 128 without spilling (2 blocks; measured faster than 80
+// registers with spills at 3 blocks); in FP32 the one-root classes fit 64 and the
+// L = 2 ones, with their compensated accumulators, 128 (2 blocks).  The other
+// classes keep ptxas's own choice (0 = no bound; an explicit 1 would let it take
+// up to 255 registers).
 template <int LA, int LB, int LC, int LD, typename R>
 __host__ __device__ constexpr int small_min_blocks() {
   constexpr int L = LA + LB + LC + LD;
-  return sizeof(R) == 8 ? (L == 0 ? LAI_MINB_L0 : L == 1 ? LAI_MINB_L1 : 0) : (L <= 1 ? LAI_MINB_F32_L1 : L == 2 ? 2 : 0);
+  return sizeof(R) == 8 ? (L == 0 ? 4 : L == 1 ? 2 : 0) : (L <= 1 ? 4 : L == 2 ? 2 : 0);
 }
 
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>

@@ -17,20 +17,14 @@ namespace lai {
 // Shared-memory table layouts, in elements of the compute type R (the FP32 kernels
 // stage FP32 copies: half the shared memory, and single-width loads).
 //
-// FP64 Boys rows hold the Taylor coefficients already divided by j!: c_j =
-// F_j(T0)/j! and d_j = F_{j+1}(T0)/j!, j < 8, so that F_0(T0 - x) = sum c_j x^j
-// and F_1(T0 - x) = sum d_j x^j are plain Horner chains (no x/j products per
-// quartet); 16 values and two pad doubles (nine 16-byte units, odd, so lanes on
-// different rows spread over the banks).  The grid stops at T0 = 38.3
-// (kBoysRowsS rows); from T = 38.3 on the asymptotic forms are used, whose
-// relative error there is below 2e-16 for F_0 and F_1 (e^-T / (2T) against
-// F_1 ~ sqrt(pi/T) / (4T)).
-#ifndef LAI_BOYS_PREDIV
-#define LAI_BOYS_PREDIV 0
-#endif
-constexpr int kBoysRowsS = LAI_BOYS_PREDIV ? 384 : kBoysNGrid;   // FP64 rows staged, T0 = k / 10
-constexpr double kBoysTmaxS = LAI_BOYS_PREDIV ? 38.3 : kBoysTmax;
-constexpr int kBoysRowS = LAI_BOYS_PREDIV ? 18 : 10;     // c_0..c_7, d_0..d_7, 2 pad | F_0..F_9
+// (A layout with the Taylor coefficients pre-divided by j!, which saves the x/j
+// products, was measured slower: its 18-double rows take more shared memory, and
+// the carve-out shrinks L1, which these kernels lean on.)
+// FP64 rows: F_0..F_9 at T0 = k / 10 (five 16-byte units, odd, so lanes on
+// different rows spread over the banks).
+constexpr int kBoysRowsS = kBoysNGrid;
+constexpr double kBoysTmaxS = kBoysTmax;
+constexpr int kBoysRowS = 10;
 constexpr int kBoysRowF = 12;     // FP32: F_0..F_11, three 16-byte units (odd)
 template <typename R>
 __host__ __device__ constexpr int boys_row() { return sizeof(R) == 8 ? kBoysRowS : kBoysRowF; }
@@ -52,24 +46,11 @@ __host__ __device__ constexpr size_t table_bytes() {
 
 template <int NR, typename R>
 __device__ __forceinline__ void stage_table(R* __restrict__ st, const RysTablesView& tab) {
-  if constexpr (NR == 1 && sizeof(R) == 8 && !LAI_BOYS_PREDIV) {
+  if constexpr (NR == 1 && sizeof(R) == 8) {
     constexpr int NV = kBoysRowS;
     for (int i = threadIdx.x; i < kBoysRowsS * NV; i += blockDim.x) {
       const int k = i / NV, j = i - k * NV;
       st[k * NV + j] = __ldg(tab.boys + k * kBoysNM + j);
-    }
-  } else if constexpr (NR == 1 && sizeof(R) == 8) {
-    constexpr int NV = kBoysRowS;
-    for (int i = threadIdx.x; i < kBoysRowsS * NV; i += blockDim.x) {
-      const int k = i / NV, j = i - k * NV;
-      // j < 8: c_j = F_j / j!; 8 <= j < 16: d_{j-8} = F_{j-7} / (j-8)!; then pad
-      const int m = j < 8 ? j : j - 8;
-      double f = 0.0;
-      if (j < 16) {
-        f = __ldg(tab.boys + k * kBoysNM + (j < 8 ? j : j - 7));
-        for (int q = 2; q <= m; ++q) f /= q;
-      }
-      st[k * NV + j] = R(f);
     }
   } else if constexpr (NR == 1) {
     constexpr int NV = boys_row<R>();  // values per row (the row holds no padding)
@@ -93,37 +74,24 @@ template <typename R>
 __device__ __forceinline__ void boys01_smem(R T, const R* __restrict__ st, R& F0, R& F1) {
   constexpr bool F64 = sizeof(R) == 8;
   if constexpr (F64) {
-    // FP64: nearest grid point by the rounding constant, Horner on the pre-divided
-    // rows (8 terms each; the first omitted term is below 6e-17 relative)
+    // FP64: nearest grid point by the rounding constant (no conversion
+    // instructions), 8-term Taylor series (first omitted term below 6e-17 relative)
     if (T < kBoysTmaxS) {
       const double km = fma(double(T), 10.0, kRoundMagicD);
       const int k = min(__double2loint(km), kBoysRowsS - 1);
       const double x = fma(km - kRoundMagicD, 0.1, -double(T));
       const double2* f = reinterpret_cast<const double2*>(st + k * kBoysRowS);
-      if constexpr (LAI_BOYS_PREDIV) {
-        const double2 c67 = f[3], d67 = f[7];
-        double a = fma(c67.y, x, c67.x), b = fma(d67.y, x, d67.x);
+      double g[10];
 #pragma unroll
-        for (int j = 2; j >= 0; --j) {
-          const double2 c = f[j], d = f[4 + j];
-          a = fma(fma(a, x, c.y), x, c.x);
-          b = fma(fma(b, x, d.y), x, d.x);
-        }
-        F0 = R(a);
-        F1 = R(b);
-      } else {
-        double g[10];
-#pragma unroll
-        for (int j = 0; j < 5; ++j) {
-          const double2 v = f[j];
-          g[2 * j] = v.x;
-          g[2 * j + 1] = v.y;
-        }
-        double a, b;
-        boys_taylor<double>(x, g, a, b);
-        F0 = R(a);
-        F1 = R(b);
+      for (int j = 0; j < 5; ++j) {
+        const double2 v = f[j];
+        g[2 * j] = v.x;
+        g[2 * j + 1] = v.y;
       }
+      double a, b;
+      boys_taylor<double>(x, g, a, b);
+      F0 = R(a);
+      F1 = R(b);
     } else {
       const R rt = fast_rsqrt(T);
       F0 = R(0.88622692545275801365) * rt;  // sqrt(pi)/2

@@ -128,29 +128,31 @@ __global__ void __launch_bounds__(kWarps * 32) eri_tiled_kernel(QuartetBlock blk
 
   const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
   const int Kab = blk.bra.Ka * blk.bra.Kb, Kcd = blk.ket.Ka * blk.ket.Kb;
-  const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
+  (void)nbra; (void)nket;
   const int W = g.LCD + 1;
   const int ncd = g.nc * g.nd, nbcd = g.nb * ncd;
   // one quartet's geometry, set per quartet below and read by the phases
-  double AB[3], CD[3];
+  double AB[3] = {0.0, 0.0, 0.0}, CD[3] = {0.0, 0.0, 0.0};
   // primitive-quartet quantities
   struct PrimQ {
     double hz, he, inv, rz, re, T, pref;
     double PA[3], QC[3], PQ[3];
   };
+  // pb, pk: the bra and ket primitive pairs' per-pair records (BraRecField); the
+  // whole warp reads the same record, a few contiguous lines
   auto prim_quartet = [&](const double* pb, const double* pk, PrimQ& o) {
-    const double zeta = __ldg(pb + PF_ZETA * sb);
-    o.hz = __ldg(pb + PF_HZ * sb);
-    const double P[3] = {__ldg(pb + PF_PX * sb), __ldg(pb + PF_PY * sb), __ldg(pb + PF_PZ * sb)};
-    o.PA[0] = __ldg(pb + PF_PAX * sb); o.PA[1] = __ldg(pb + PF_PAY * sb); o.PA[2] = __ldg(pb + PF_PAZ * sb);
-    const double cab = __ldg(pb + PF_C * sb);
-    const double eta = __ldg(pk + PF_ZETA * sk);
-    o.he = __ldg(pk + PF_HZ * sk);
-    o.QC[0] = __ldg(pk + PF_PAX * sk); o.QC[1] = __ldg(pk + PF_PAY * sk); o.QC[2] = __ldg(pk + PF_PAZ * sk);
-    o.PQ[0] = P[0] - __ldg(pk + PF_PX * sk);
-    o.PQ[1] = P[1] - __ldg(pk + PF_PY * sk);
-    o.PQ[2] = P[2] - __ldg(pk + PF_PZ * sk);
-    const double ccd = __ldg(pk + PF_C * sk);
+    const double zeta = __ldg(pb + BR_ZETA);
+    o.hz = __ldg(pb + BR_HZ);
+    const double P[3] = {__ldg(pb + BR_PX), __ldg(pb + BR_PY), __ldg(pb + BR_PZ)};
+    o.PA[0] = __ldg(pb + BR_PAX); o.PA[1] = __ldg(pb + BR_PAY); o.PA[2] = __ldg(pb + BR_PAZ);
+    const double cab = __ldg(pb + BR_C);
+    const double eta = __ldg(pk + BR_ZETA);
+    o.he = __ldg(pk + BR_HZ);
+    o.QC[0] = __ldg(pk + BR_PAX); o.QC[1] = __ldg(pk + BR_PAY); o.QC[2] = __ldg(pk + BR_PAZ);
+    o.PQ[0] = P[0] - __ldg(pk + BR_PX);
+    o.PQ[1] = P[1] - __ldg(pk + BR_PY);
+    o.PQ[2] = P[2] - __ldg(pk + BR_PZ);
+    const double ccd = __ldg(pk + BR_C);
     const double rs = rsqrt(zeta + eta);
     o.inv = rs * rs;
     o.rz = eta * o.inv;
@@ -292,9 +294,9 @@ __global__ void __launch_bounds__(kWarps * 32) eri_tiled_kernel(QuartetBlock blk
         // one primitive quartet and one root batch: its tables, built in the first
         // pass, stay in shared memory for the later passes
         if (pass == 0) {
-          const double* pb = blk.bra.prim + p;
-          const double* pk = blk.ket.prim + q;
-          const double qab = __ldg(pb + PF_Q * sb), qcd = __ldg(pk + PF_Q * sk);
+          const double* pb = blk.bra.primb + (size_t)p * Kab * kBraRec;
+          const double* pk = blk.ket.primb + (size_t)q * Kcd * kBraRec;
+          const double qab = __ldg(pb + BR_Q), qcd = __ldg(pk + BR_Q);
           have_tables = !(qab * qcd < args.prim_eps);
           if (have_tables) {
             ++nprim_done;
@@ -307,12 +309,12 @@ __global__ void __launch_bounds__(kWarps * 32) eri_tiled_kernel(QuartetBlock blk
         if (have_tables) output_phase(g.n, off, acc);
       } else {
         for (int ib = 0; ib < Kab; ++ib) {
-          const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
-          const double qab = __ldg(pb + PF_Q * sb);
+          const double* pb = blk.bra.primb + ((size_t)p * Kab + ib) * kBraRec;
+          const double qab = __ldg(pb + BR_Q);
           if (qab * blk.ket.qprim_max < args.prim_eps) break;
           for (int ik = 0; ik < Kcd; ++ik) {
-            const double* pk = blk.ket.prim + (size_t)ik * nket + q;
-            const double qcd = __ldg(pk + PF_Q * sk);
+            const double* pk = blk.ket.primb + ((size_t)q * Kcd + ik) * kBraRec;
+            const double qcd = __ldg(pk + BR_Q);
             if (qab * qcd < args.prim_eps) break;
             if (pass == 0) ++nprim_done;
             PrimQ pq;

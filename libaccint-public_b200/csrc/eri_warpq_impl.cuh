@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
 
   const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
   const int Kab = blk.bra.Ka * blk.bra.Kb, Kcd = blk.ket.Ka * blk.ket.Kb;
-  const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
+  (void)nbra; (void)nket;
 
   const int64_t gw = (int64_t)blockIdx.x * kWarpqWarps + warp;
   const int64_t nw = (int64_t)gridDim.x * kWarpqWarps;
@@ -266,23 +266,29 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
 #pragma unroll
     for (int m = 0; m < MG; ++m) G[m] = 0.0;
 
+    // the whole warp works on one quartet: bra and ket primitives come from their
+    // per-pair records (a few contiguous lines per pair, 16-byte loads)
+    const double2* rbp = reinterpret_cast<const double2*>(blk.bra.primb + (size_t)p * Kab * kBraRec);
+    const double2* rkp = reinterpret_cast<const double2*>(blk.ket.primb + (size_t)q * Kcd * kBraRec);
     for (int ib = 0; ib < Kab; ++ib) {
-      const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
-      const double qab = __ldg(pb + PF_Q * sb);
+      const double2* rb = rbp + ib * (kBraRec / 2);
+      const double2 b0 = __ldg(rb), b1 = __ldg(rb + 1);
+      const double qab = b0.x;
       if (qab * blk.ket.qprim_max < args.prim_eps) break;
-      const double zeta = __ldg(pb + PF_ZETA * sb), hz = __ldg(pb + PF_HZ * sb);
-      const double Px = __ldg(pb + PF_PX * sb), Py = __ldg(pb + PF_PY * sb), Pz = __ldg(pb + PF_PZ * sb);
-      const double PAx = __ldg(pb + PF_PAX * sb), PAy = __ldg(pb + PF_PAY * sb), PAz = __ldg(pb + PF_PAZ * sb);
-      const double cab = __ldg(pb + PF_C * sb);
+      const double2 b2 = __ldg(rb + 2), b3 = __ldg(rb + 3), b4 = __ldg(rb + 4), b5 = __ldg(rb + 5);
+      const double zeta = b0.y, hz = b1.x, cab = b1.y;
+      const double Px = b2.x, Py = b2.y, Pz = b3.x;
+      const double PAx = b4.x, PAy = b4.y, PAz = b5.x;
       for (int ik = 0; ik < Kcd; ++ik) {
-        const double* pk = blk.ket.prim + (size_t)ik * nket + q;
-        const double qcd = __ldg(pk + PF_Q * sk);
+        const double2* rk = rkp + ik * (kBraRec / 2);
+        const double2 k0 = __ldg(rk);
+        const double qcd = k0.x;
         if (qab * qcd < args.prim_eps) break;
         ++nprim_done;
-        const double eta = __ldg(pk + PF_ZETA * sk), he = __ldg(pk + PF_HZ * sk);
-        const double PQx = Px - __ldg(pk + PF_PX * sk), PQy = Py - __ldg(pk + PF_PY * sk),
-                     PQz = Pz - __ldg(pk + PF_PZ * sk);
-        const double ccd = __ldg(pk + PF_C * sk);
+        const double2 k1 = __ldg(rk + 1), k2 = __ldg(rk + 2), k3 = __ldg(rk + 3);
+        const double eta = k0.y, he = k1.x, ccd = k1.y;
+        const double PQx = Px - k2.x, PQy = Py - k2.y, PQz = Pz - k3.x;
+        const double* pkr = reinterpret_cast<const double*>(rk);
         const double rs = rsqrt(zeta + eta);
         const double inv = rs * rs;
         const double rz = eta * inv, re = zeta * inv;
@@ -294,8 +300,7 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
           rys_root_one<double>(NR, r, T, tab, u, w);
           const double pqx = x == 0 ? PQx : x == 1 ? PQy : PQz;
           const double pax = x == 0 ? PAx : x == 1 ? PAy : PAz;
-          const double qcx = x == 0 ? __ldg(pk + PF_PAX * sk) : x == 1 ? __ldg(pk + PF_PAY * sk)
-                                                                    : __ldg(pk + PF_PAZ * sk);
+          const double qcx = __ldg(pkr + BR_PAX + x);
           const double pa = pax - rz * u * pqx;
           const double qc = qcx + re * u * pqx;
           const double b00 = 0.5 * inv * u, b10 = hz - hz * rz * u, b01 = he - he * re * u;
