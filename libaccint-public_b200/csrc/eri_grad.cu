@@ -18,10 +18,14 @@
 // horizontal transfer I(a, b+1) = I(a+1, b) + AB_x I(a, b) on both sides; the
 // root count is that of total angular momentum L+1.
 //
-// One warp per quartet: lanes 0..2 build the three directions' tables in shared
-// memory, then all lanes sweep the quartet's Cartesian components, each keeping
-// nine partial derivatives (A, B, C x xyz), reduced over the warp at the end.
+// One warp per quartet: lanes 3 r + x build the tables of root r and direction x in
+// shared memory (all roots at once where shared memory allows), then all lanes
+// sweep the quartet's Cartesian components over those roots, each keeping nine
+// partial derivatives (A, B, C x xyz), reduced over the warp at the end.  (The low
+// classes run on the thread-per-quartet kernels of eri_grad_small.cuh.)
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "eri_device.cuh"
 #include "eri_kernels.h"
@@ -39,6 +43,7 @@ struct GradGeom {
   int vsz, xsz, hsz;       // (LABp+1)(LCDp+1), EA*EB*(LCDp+1), EA*EB*EC*ED
   int off_v, off_x, off_h, off_g, per_warp;  // shared memory per warp (doubles)
   int gamma_global;        // G_abcd kept in global scratch instead of shared memory
+  int rb;                  // roots whose tables are built at once (lanes 3 r + x, r < rb)
 };
 
 GradGeom make_grad_geom(int la, int lb, int lc, int ld, int warps, size_t smem_max) {
@@ -52,16 +57,20 @@ GradGeom make_grad_geom(int la, int lb, int lc, int ld, int warps, size_t smem_m
   g.vsz = (g.LABp + 1) * (g.LCDp + 1);
   g.xsz = g.EA * g.EB * (g.LCDp + 1);
   g.hsz = g.EA * g.EB * g.EC * g.ED;
-  for (int glob = 0; glob <= 1; ++glob) {
-    int o = 0;
-    g.off_v = o; o += 3 * g.vsz;
-    g.off_x = o; o += 3 * g.xsz;
-    g.off_h = o; o += 3 * g.hsz;
-    g.off_g = o; o += glob ? 0 : g.nel;
-    g.per_warp = (o + 1) & ~1;
-    g.gamma_global = glob;
-    if ((size_t)g.per_warp * 8 * warps <= smem_max) return g;
-  }
+  // as many roots at once as shared memory allows (all of them for l <= 2), G in
+  // shared memory if it fits beside them
+  for (int rb = std::min(g.n, 10); rb >= 1; --rb)
+    for (int glob = 0; glob <= 1; ++glob) {
+      int o = 0;
+      g.off_v = o; o += 3 * rb * g.vsz;
+      g.off_x = o; o += 3 * rb * g.xsz;
+      g.off_h = o; o += 3 * rb * g.hsz;
+      g.off_g = o; o += glob ? 0 : g.nel;
+      g.per_warp = (o + 1) & ~1;
+      g.gamma_global = glob;
+      g.rb = rb;
+      if ((size_t)g.per_warp * 8 * warps <= smem_max) return g;
+    }
   g.per_warp = -1;
   return g;
 }
@@ -148,15 +157,16 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(QuartetBlock blk, GradArg
         const double pref = cab * ccd * rs;
         double u[kMaxRoots + 1], w[kMaxRoots + 1];
         rys_roots_table<double>(g.n, T, tab, u, w);
-        for (int r = 0; r < g.n; ++r) {
-          const double ur = u[r];
-          if (lane < 3) {  // vertical recurrence, direction x = lane
-            const int x = lane;
-            double* I = V + x * g.vsz;
+        for (int r0 = 0; r0 < g.n; r0 += g.rb) {
+          const int nr = min(g.rb, g.n - r0);
+          if (lane < 3 * nr) {  // vertical recurrence and transfers of root r0 + lane / 3, direction lane % 3
+            const int rr = lane / 3, x = lane - 3 * rr;
+            const double ur = u[r0 + rr];
+            double* I = V + (rr * 3 + x) * g.vsz;
             const double b00 = 0.5 * inv * ur, b10 = hz - hz * rz * ur, b01 = he - he * re * ur;
             const double pa = PA[x] - rz * ur * PQ[x];
             const double qc = QC[x] + re * ur * PQ[x];
-            I[0] = (x == 2) ? w[r] * pref : 1.0;
+            I[0] = (x == 2) ? w[r0 + rr] * pref : 1.0;
             if (g.LABp > 0) I[W] = pa * I[0];
             for (int e = 1; e < g.LABp; ++e) I[(e + 1) * W] = pa * I[e * W] + e * b10 * I[(e - 1) * W];
             for (int f = 0; f < g.LCDp; ++f)
@@ -168,7 +178,7 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(QuartetBlock blk, GradArg
               }
             // horizontal transfer, bra then ket: X[a][b][f] (a < EA, b < EB), then
             // H[a][b][c][d] (c < EC, d < ED); I(a, b+1) = I(a+1, b) + AB I(a, b)
-            double* Xx = X + x * g.xsz;
+            double* Xx = X + (rr * 3 + x) * g.xsz;
             const int F = g.LCDp + 1;
             for (int f = 0; f <= g.LCDp; ++f) {
               double row[12];
@@ -179,7 +189,7 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(QuartetBlock blk, GradArg
                 for (int a = 0; a < g.EA && a + b <= g.LABp; ++a) Xx[(a * g.EB + b) * F + f] = row[a];
               }
             }
-            double* Hx = H + x * g.hsz;
+            double* Hx = H + (rr * 3 + x) * g.hsz;
             for (int a = 0; a < g.EA; ++a)
               for (int b = 0; b < g.EB && a + b <= g.LABp; ++b) {
                 double col[12];
@@ -192,9 +202,6 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(QuartetBlock blk, GradArg
               }
           }
           __syncwarp();
-          const double* Hx = H;
-          const double* Hy = H + g.hsz;
-          const double* Hz = H + 2 * g.hsz;
           const double al2 = 2.0 * alpha, be2 = 2.0 * beta, ga2 = 2.0 * gamma;
           for (int e = lane; e < g.nel; e += 32) {
             const int d = e % g.nd, c = (e / g.nd) % g.nc, b = (e / (g.nd * g.nc)) % g.nb,
@@ -205,22 +212,23 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(QuartetBlock blk, GradArg
             const int B[3] = {comp_x(cb), comp_y(cb), comp_z(cb)};
             const int C[3] = {comp_x(cc), comp_y(cc), comp_z(cc)};
             const int Dd[3] = {comp_x(cd), comp_y(cd), comp_z(cd)};
-            const double* Hd[3] = {Hx, Hy, Hz};
-            double base[3], dA[3], dB[3], dC[3];
-#pragma unroll
-            for (int x = 0; x < 3; ++x) {
-              const double* h = Hd[x];
-              const int ax = A[x], bx = B[x], cx = C[x], dx = Dd[x];
-              base[x] = h[hidx(g, ax, bx, cx, dx)];
-              dA[x] = al2 * h[hidx(g, ax + 1, bx, cx, dx)] - (ax ? ax * h[hidx(g, ax - 1, bx, cx, dx)] : 0.0);
-              dB[x] = be2 * h[hidx(g, ax, bx + 1, cx, dx)] - (bx ? bx * h[hidx(g, ax, bx - 1, cx, dx)] : 0.0);
-              dC[x] = ga2 * h[hidx(g, ax, bx, cx + 1, dx)] - (cx ? cx * h[hidx(g, ax, bx, cx - 1, dx)] : 0.0);
-            }
             const double gm = Gam[e];
-            const double pyz = base[1] * base[2], pxz = base[0] * base[2], pxy = base[0] * base[1];
-            acc[0] += gm * dA[0] * pyz; acc[1] += gm * dA[1] * pxz; acc[2] += gm * dA[2] * pxy;
-            acc[3] += gm * dB[0] * pyz; acc[4] += gm * dB[1] * pxz; acc[5] += gm * dB[2] * pxy;
-            acc[6] += gm * dC[0] * pyz; acc[7] += gm * dC[1] * pxz; acc[8] += gm * dC[2] * pxy;
+            for (int rr = 0; rr < nr; ++rr) {
+              double base[3], dA[3], dB[3], dC[3];
+#pragma unroll
+              for (int x = 0; x < 3; ++x) {
+                const double* h = H + (rr * 3 + x) * g.hsz;
+                const int ax = A[x], bx = B[x], cx = C[x], dx = Dd[x];
+                base[x] = h[hidx(g, ax, bx, cx, dx)];
+                dA[x] = al2 * h[hidx(g, ax + 1, bx, cx, dx)] - (ax ? ax * h[hidx(g, ax - 1, bx, cx, dx)] : 0.0);
+                dB[x] = be2 * h[hidx(g, ax, bx + 1, cx, dx)] - (bx ? bx * h[hidx(g, ax, bx - 1, cx, dx)] : 0.0);
+                dC[x] = ga2 * h[hidx(g, ax, bx, cx + 1, dx)] - (cx ? cx * h[hidx(g, ax, bx, cx - 1, dx)] : 0.0);
+              }
+              const double pyz = base[1] * base[2], pxz = base[0] * base[2], pxy = base[0] * base[1];
+              acc[0] += gm * dA[0] * pyz; acc[1] += gm * dA[1] * pxz; acc[2] += gm * dA[2] * pxy;
+              acc[3] += gm * dB[0] * pyz; acc[4] += gm * dB[1] * pxz; acc[5] += gm * dB[2] * pxy;
+              acc[6] += gm * dC[0] * pyz; acc[7] += gm * dC[1] * pxz; acc[8] += gm * dC[2] * pxy;
+            }
           }
           __syncwarp();
         }

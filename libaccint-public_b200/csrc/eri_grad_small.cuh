@@ -21,11 +21,12 @@
 
 #include "eri_device.cuh"
 #include "eri_kernels.h"
+#include "eri_tables_smem.cuh"
 
 namespace lai {
 namespace grad_small {
 
-enum { DA = 0, DB = 1, DC = 2 };
+enum { DA = 0, DB = 1, DC = 2, DAB = 3 };  // DAB: the A and B centres in one pass
 
 template <int B, int E, typename F>
 __device__ __forceinline__ void gfor(F&& f) {
@@ -81,47 +82,74 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
   constexpr int LAB = LA + LB, LCD = LC + LD;
   constexpr int NR = (LAB + LCD + 1) / 2 + 1;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-  // raised block W and lowered block U, as shell ranges [E0, E1] x [F0, F1]
-  constexpr int WE0 = DER == DA ? LA + 1 : LA, WE1 = DER == DC ? LAB : LAB + 1;
+  // raised block W (W2: the B block of a merged A+B pass) and lowered block U, as
+  // shell ranges [E0, E1] x [F0, F1]
+  constexpr bool AB_ = DER == DAB;
+  constexpr int WE0 = (DER == DA || AB_) ? LA + 1 : LA, WE1 = DER == DC ? LAB : LAB + 1;
   constexpr int WF0 = DER == DC ? LC + 1 : LC, WF1 = DER == DC ? LCD + 1 : LCD;
-  constexpr bool HAS_U = DER == DA ? LA >= 1 : DER == DB ? LB >= 1 : LC >= 1;
-  constexpr int UE0 = DER == DA ? (LA >= 1 ? LA - 1 : 0) : LA;
-  constexpr int UE1 = DER == DA ? LAB - 1 : DER == DB ? LAB - 1 : LAB;
+  constexpr bool HAS_U = DER == DA ? LA >= 1 : DER == DB ? LB >= 1 : DER == DC ? LC >= 1 : (LA >= 1 || LB >= 1);
+  constexpr int UE0 = (DER == DA || AB_) ? (LA >= 1 ? LA - 1 : 0) : LA;
+  constexpr int UE1 = DER == DC ? LAB : LAB - 1;
   constexpr int UF0 = DER == DC ? (LC >= 1 ? LC - 1 : 0) : LC;
   constexpr int UF1 = DER == DC ? LCD - 1 : LCD;
   constexpr int NWE = ncart_range(WE0, WE1), NWF = ncart_range(WF0, WF1);
+  constexpr int NW2E = AB_ ? ncart_range(LA, LAB + 1) : 1;  // W2: e in [LA, LAB+1], f as W
   constexpr int NUE = HAS_U ? ncart_range(UE0, UE1) : 1, NUF = HAS_U ? ncart_range(UF0, UF1) : 1;
   constexpr int EM = DER == DC ? LAB : LAB + 1;  // vertical recurrence extents
   constexpr int FM = DER == DC ? LCD + 1 : LCD;
 
+  // the Boys grid / the Rys fit table of NR roots, staged once per block (per-lane
+  // gathers from global memory would touch up to 32 lines per load)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* stab = reinterpret_cast<double*>(smem_raw);
+  stage_table<NR, double>(stab, tab);
+  __syncthreads();
   const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
   const int Kab = blk.bra.Ka * blk.bra.Kb, Kcd = blk.ket.Ka * blk.ket.Kb;
   const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
-  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t t = blk.t_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < blk.total; t += nthreads) {
-    const int p = find_bra(blk.offsets, nbra, t);
+  // warps take chunks of 32 consecutive quartets (grid-stride); one bra search per
+  // chunk, then each lane steps forward to its own bra pair (usually the same)
+  const int lane = threadIdx.x & 31;
+  const int64_t nq = blk.total - blk.t_begin;
+  const int64_t nchunks = (nq + 31) / 32;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t ch = wid; ch < nchunks; ch += nw) {
+    const int64_t t0 = blk.t_begin + ch * 32;
+    const int64_t t = t0 + lane;
+    int pw = 0;
+    if (lane == 0) pw = find_bra(blk.offsets, nbra, t0);
+    pw = __shfl_sync(0xffffffffu, pw, 0);
+    if (t >= blk.total) continue;
+    int p = pw;
+    while (t >= __ldg(blk.offsets + p + 1)) ++p;
     const int q = (blk.qbegin ? __ldg(blk.qbegin + p) : 0) + (int)(t - __ldg(blk.offsets + p));
-    double W[NWE * NWF], U[NUE * NUF];
+    double W[NWE * NWF], W2[AB_ ? NW2E * NWF : 1], U[NUE * NUF];
 #pragma unroll
     for (int i = 0; i < NWE * NWF; ++i) W[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < (AB_ ? NW2E * NWF : 1); ++i) W2[i] = 0.0;
 #pragma unroll
     for (int i = 0; i < NUE * NUF; ++i) U[i] = 0.0;
 
     for (int ib = 0; ib < Kab; ++ib) {
-      const double* pb = blk.bra.prim + (size_t)ib * nbra + p;
-      const double qab = __ldg(pb + PF_Q * sb);
+      // bra primitive: its per-pair record (the warp usually shares the bra pair);
+      // the exponent on A from the SoA table
+      const double2* rb = reinterpret_cast<const double2*>(blk.bra.primb + ((size_t)p * Kab + ib) * kBraRec);
+      const double2 b0 = __ldg(rb), b1 = __ldg(rb + 1);
+      const double qab = b0.x;
       if (qab * blk.ket.qprim_max < ga.prim_eps) break;
-      const double zeta = __ldg(pb + PF_ZETA * sb), hz = __ldg(pb + PF_HZ * sb);
-      const double alpha = __ldg(pb + PF_ALPHA * sb);
-      const double P[3] = {__ldg(pb + PF_PX * sb), __ldg(pb + PF_PY * sb), __ldg(pb + PF_PZ * sb)};
-      const double PA[3] = {__ldg(pb + PF_PAX * sb), __ldg(pb + PF_PAY * sb), __ldg(pb + PF_PAZ * sb)};
-      const double cab = __ldg(pb + PF_C * sb);
+      const double2 b2 = __ldg(rb + 2), b3 = __ldg(rb + 3), b4 = __ldg(rb + 4), b5 = __ldg(rb + 5);
+      const double zeta = b0.y, hz = b1.x, cab = b1.y;
+      const double alpha = DER != DC ? __ldg(blk.bra.prim + (size_t)ib * nbra + p + PF_ALPHA * sb) : 0.0;
+      const double P[3] = {b2.x, b2.y, b3.x};
+      const double PA[3] = {b4.x, b4.y, b5.x};
       for (int ik = 0; ik < Kcd; ++ik) {
         const double* pk = blk.ket.prim + (size_t)ik * nket + q;
         const double qcd = __ldg(pk + PF_Q * sk);
         if (qab * qcd < ga.prim_eps) break;
         const double eta = __ldg(pk + PF_ZETA * sk), he = __ldg(pk + PF_HZ * sk);
-        const double gamma = __ldg(pk + PF_ALPHA * sk);
+        const double gamma = DER == DC ? __ldg(pk + PF_ALPHA * sk) : 0.0;
         const double PQ[3] = {P[0] - __ldg(pk + PF_PX * sk), P[1] - __ldg(pk + PF_PY * sk),
                               P[2] - __ldg(pk + PF_PZ * sk)};
         const double QC[3] = {__ldg(pk + PF_PAX * sk), __ldg(pk + PF_PAY * sk), __ldg(pk + PF_PAZ * sk)};
@@ -131,9 +159,10 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
         const double rz = eta * inv, re = zeta * inv;
         const double T = zeta * rz * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
         const double pref = cab * ccd * rs;
-        const double kap2 = 2.0 * (DER == DA ? alpha : DER == DB ? zeta - alpha : gamma);
+        const double kap2 = 2.0 * ((DER == DA || AB_) ? alpha : DER == DB ? zeta - alpha : gamma);
+        const double kapb2 = 2.0 * (zeta - alpha);  // the B block of a merged pass
         double u[NR], w[NR];
-        rys_roots_table<double>(NR, T, tab, u, w);
+        rys_smem<NR, double>(T, stab, tab, u, w);
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
           const double ur = u[r];
@@ -154,6 +183,24 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
                 I[x][e][f + 1] = qc * I[x][e][f] + (f ? f * b01 * I[x][e][f > 0 ? f - 1 : 0] : 0.0) +
                                  (e ? e * b00 * I[x][e > 0 ? e - 1 : 0][f] : 0.0);
           }
+          if constexpr (AB_) {
+            // merged A+B pass: the products over e in [LA, LAB+1] once, into the B
+            // block (2 beta) and, for e >= LA+1, the A block (2 alpha)
+            gfor<0, NW2E>([&](auto IE) {
+              constexpr int ie = decltype(IE)::value;
+              constexpr int le = [] { int l = LA, r = ie; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
+              constexpr int ce = cart_comp(le, ie - ncart_before(LA, le));
+              gfor<0, NWF>([&](auto JF) {
+                constexpr int jf = decltype(JF)::value;
+                constexpr int lf = [] { int l = WF0, r = jf; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
+                constexpr int cf = cart_comp(lf, jf - ncart_before(WF0, lf));
+                const double X = I[0][comp_x(ce)][comp_x(cf)] * I[1][comp_y(ce)][comp_y(cf)] *
+                                 I[2][comp_z(ce)][comp_z(cf)];
+                W2[ie * NWF + jf] += kapb2 * X;
+                if constexpr (ie >= ncart(LA)) W[(ie - ncart(LA)) * NWF + jf] += kap2 * X;
+              });
+            });
+          } else
           // raised block
           gfor<0, NWE>([&](auto IE) {
             constexpr int ie = decltype(IE)::value;
@@ -190,7 +237,7 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
                  ABz = __ldg(blk.bra.AB + 2 * nbra + p);
     const double CDx = __ldg(blk.ket.AB + q), CDy = __ldg(blk.ket.AB + nket + q),
                  CDz = __ldg(blk.ket.AB + 2 * nket + q);
-    constexpr int PB = LB + (DER == DB ? 1 : 0), PD = LD;
+    constexpr int PB = LB + ((DER == DB || AB_) ? 1 : 0), PD = LD;
     double abp[3][PB + 1], cdp[3][PD + 1];
     abp[0][0] = abp[1][0] = abp[2][0] = 1.0;
     cdp[0][0] = cdp[1][0] = cdp[2][0] = 1.0;
@@ -207,7 +254,8 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
     const double s = quartet_weight(blk, p, q);
     const double* __restrict__ D = ga.D;
     const size_t nbf = (size_t)ga.nbf;
-    double g[3] = {0.0, 0.0, 0.0};
+    double g[3] = {0.0, 0.0, 0.0}, g2[3] = {0.0, 0.0, 0.0};  // g2: the B centre of a merged pass
+    constexpr int D1 = AB_ ? DA : DER;  // the centre g belongs to
     gfor<0, NA>([&](auto IA) {
       constexpr int a = decltype(IA)::value;
       constexpr int ca = cart_comp(LA, a);
@@ -233,9 +281,9 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
             gfor<0, 3>([&](auto X) {
               constexpr int x = decltype(X)::value;
               // raised term: component shifted by +1 in x on the derivative centre
-              constexpr int ra = DER == DA ? shift(ca, x, 1) : ca;
-              constexpr int rb = DER == DB ? shift(cb, x, 1) : cb;
-              constexpr int rc = DER == DC ? shift(cc, x, 1) : cc;
+              constexpr int ra = D1 == DA ? shift(ca, x, 1) : ca;
+              constexpr int rb = D1 == DB ? shift(cb, x, 1) : cb;
+              constexpr int rc = D1 == DC ? shift(cc, x, 1) : cc;
               double acc = 0.0;
               hrr_terms<ra, rb, WE0>(abp, [&](auto E, double hb) {
                 hrr_terms<rc, cd, WF0>(cdp, [&](auto F, double hd) {
@@ -243,11 +291,11 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
                 });
               });
               // lowered term: - n_x times the component shifted by -1
-              constexpr int nx = comp_n(DER == DA ? ca : DER == DB ? cb : cc, x);
+              constexpr int nx = comp_n(D1 == DA ? ca : D1 == DB ? cb : cc, x);
               if constexpr (HAS_U && nx > 0) {
-                constexpr int la_ = DER == DA ? shift(ca, x, -1) : ca;
-                constexpr int lb_ = DER == DB ? shift(cb, x, -1) : cb;
-                constexpr int lc_ = DER == DC ? shift(cc, x, -1) : cc;
+                constexpr int la_ = D1 == DA ? shift(ca, x, -1) : ca;
+                constexpr int lb_ = D1 == DB ? shift(cb, x, -1) : cb;
+                constexpr int lc_ = D1 == DC ? shift(cc, x, -1) : cc;
                 double low = 0.0;
                 hrr_terms<la_, lb_, UE0>(abp, [&](auto E, double hb) {
                   hrr_terms<lc_, cd, UF0>(cdp, [&](auto F, double hd) {
@@ -257,19 +305,43 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
                 acc -= nx * low;
               }
               g[x] += G * acc;
+              if constexpr (AB_) {  // the B centre: W2 over e in [LA, LAB+1], U for b - 1x
+                double accb = 0.0;
+                hrr_terms<ca, shift(cb, x, 1), LA>(abp, [&](auto E, double hb) {
+                  hrr_terms<cc, cd, WF0>(cdp, [&](auto F, double hd) {
+                    accb += hb * hd * W2[decltype(E)::value * NWF + decltype(F)::value];
+                  });
+                });
+                constexpr int nbx = comp_n(cb, x);
+                if constexpr (HAS_U && nbx > 0) {
+                  double low = 0.0;
+                  hrr_terms<ca, shift(cb, x, -1), UE0>(abp, [&](auto E, double hb) {
+                    hrr_terms<cc, cd, UF0>(cdp, [&](auto F, double hd) {
+                      low += hb * hd * U[decltype(E)::value * NUF + decltype(F)::value];
+                    });
+                  });
+                  accb -= nbx * low;
+                }
+                g2[x] += G * accb;
+              }
             });
           });
         });
       });
     });
-    const int sh = DER == DA ? __ldg(blk.bra.shell_a + p) : DER == DB ? __ldg(blk.bra.shell_b + p)
-                                                                      : __ldg(blk.ket.shell_a + q);
+    const int sh = D1 == DA ? __ldg(blk.bra.shell_a + p) : D1 == DB ? __ldg(blk.bra.shell_b + p)
+                                                                    : __ldg(blk.ket.shell_a + q);
     const int at = __ldg(ga.shell_atom + sh);
     const int atD = __ldg(ga.shell_atom + __ldg(blk.ket.shell_b + q));
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
       atomicAdd(ga.grad + 3 * at + x, g[x]);
-      atomicAdd(ga.grad + 3 * atD + x, -g[x]);
+      atomicAdd(ga.grad + 3 * atD + x, -(g[x] + g2[x]));
+    }
+    if constexpr (AB_) {
+      const int atB = __ldg(ga.shell_atom + __ldg(blk.bra.shell_b + p));
+#pragma unroll
+      for (int x = 0; x < 3; ++x) atomicAdd(ga.grad + 3 * atB + x, g2[x]);
     }
   }
 }
@@ -279,12 +351,37 @@ int launch(const QuartetBlock& blk, const GradSmallArgs& ga, const RysTablesView
            int num_sms) {
   const int64_t nq = blk.total - blk.t_begin;
   if (nq <= 0) return 0;
+  constexpr int NR = (LA + LB + LC + LD + 1) / 2 + 1;
+  // the A and B centres in one pass when its three accumulator blocks stay small
+  constexpr int LAB = LA + LB, LCD = LC + LD;
+  constexpr int nf = ncart_range(LC, LCD);
+  constexpr int merged_size = (ncart_range(LA + 1, LAB + 1) + ncart_range(LA, LAB + 1) +
+                               ((LA >= 1 || LB >= 1) ? ncart_range(LA >= 1 ? LA - 1 : 0, LAB - 1) : 0)) * nf;
+  constexpr bool kMerge = merged_size <= 40;
+  const size_t smem = table_bytes<NR, double>();
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(grad_small_kernel<LA, LB, LC, LD, DA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(grad_small_kernel<LA, LB, LC, LD, DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(grad_small_kernel<LA, LB, LC, LD, DC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        (kMerge && cudaFuncSetAttribute(grad_small_kernel<LA, LB, LC, LD, DAB>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess))
+      return -3;
+    attr = true;
+  }
   const int threads = 128;
   const int64_t want = (nq + threads - 1) / threads;
   const int grid = (int)(want < (int64_t)num_sms * 8 ? want : (int64_t)num_sms * 8);
-  grad_small_kernel<LA, LB, LC, LD, DA><<<grid, threads, 0, stream>>>(blk, ga, tab);
-  grad_small_kernel<LA, LB, LC, LD, DB><<<grid, threads, 0, stream>>>(blk, ga, tab);
-  grad_small_kernel<LA, LB, LC, LD, DC><<<grid, threads, 0, stream>>>(blk, ga, tab);
+  if constexpr (kMerge) {
+    grad_small_kernel<LA, LB, LC, LD, DAB><<<grid, threads, smem, stream>>>(blk, ga, tab);
+  } else {
+    grad_small_kernel<LA, LB, LC, LD, DA><<<grid, threads, smem, stream>>>(blk, ga, tab);
+    grad_small_kernel<LA, LB, LC, LD, DB><<<grid, threads, smem, stream>>>(blk, ga, tab);
+  }
+  grad_small_kernel<LA, LB, LC, LD, DC><<<grid, threads, smem, stream>>>(blk, ga, tab);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 
