@@ -601,7 +601,8 @@ __device__ __forceinline__ void small_finish(GV&& gval, const QuartetBlock& blk,
 // registers with spills at 3 blocks); in FP32 the one-root classes fit 64 and the
 // L = 2 ones, with their compensated accumulators, 128 (2 blocks).  The other
 // classes keep ptxas's own choice (0 = no bound; an explicit 1 would let it take
-// up to 255 registers).
+// up to 255 registers): capping the L = 3 and 4 classes at 128 registers (2
+// blocks) measured slower in both precisions, (pp|ps) FP64 127 -> 154 ms.
 template <int LA, int LB, int LC, int LD, typename R>
 __host__ __device__ constexpr int small_min_blocks() {
   constexpr int L = LA + LB + LC + LD;

@@ -186,6 +186,21 @@ def test_gradient_h2o16_device_time(lai):
     print(f"(H2O)16/cc-pVDZ: J/K build {out['jk']:.2f} ms, gradient {out['gradient']:.2f} ms")
     assert np.max(np.abs(G.sum(dim=0).cpu().numpy())) < 1e-8
 
+
+def test_gradient_f_shells_vs_finite_differences(lai):
+    """H2O / cc-pVTZ (f on O, d on H): the warp-per-quartet gradient kernel on the
+    classes above d, and the thread-per-quartet ones on the rest, against central
+    differences of our energy (no screening) on three coordinates."""
+    w = lai.workloads.make("h2o1_ccpvtz")
+    assert max(s.l for s in w.basis.shells) == 3
+    g = _grad(lai, w.Z, w.xyz, w.D, "cc-pvtz")
+    assert np.max(np.abs(g.sum(axis=0))) < 1e-9
+    for a, x in [(0, 0), (1, 1), (2, 2)]:
+        xp = w.xyz.copy(); xp[a, x] += H
+        xm = w.xyz.copy(); xm[a, x] -= H
+        fd = (_energy(lai, w.Z, xp, w.D, "cc-pvtz") - _energy(lai, w.Z, xm, w.D, "cc-pvtz")) / (2 * H)
+        assert abs(g[a, x] - fd) < GRAD_TOL, (a, x, g[a, x], fd)
+
 def test_gradient_requires_atoms(lai):
     w = lai.workloads.make("h2o1_sto3g")
     shells = [lai.Shell(s.l, s.center, s.exps, s.coefs) for s in w.basis.shells]  # atom = -1
