@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define LAI_ABI_VERSION 1
+#define LAI_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define LAI_API __attribute__((visibility("default")))
@@ -140,6 +140,14 @@ typedef struct {
                           launch instead of one per shell-quartet class).  Needs
                           a non-NULL stream and profile = 0; the replays keep
                           the FP32 cut derived from max|D| at capture time.     */
+  double fp32_prim_rel; /* mixed precision, FP32 quartets only: also skip their
+                          primitive quartets whose bound q_ab*q_cd is below
+                          fp32_prim_rel * Q_ij*Q_kl (the quartet's own Schwarz
+                          bound), so that each skipped term is below that
+                          fraction of the quartet -- primitive accuracy matched
+                          to the FP32 arithmetic.  0 = off (the engine's
+                          absolute primitive cut only).  No counterpart in the
+                          reference.                                            */
 } lai_jk_opts;
 LAI_API void lai_jk_opts_default(lai_jk_opts* opts);
 /* The slice [lo, hi) of a block of `total` quartets that shard `index` of `count`

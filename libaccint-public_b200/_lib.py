@@ -49,7 +49,7 @@ class EngineOpts(ctypes.Structure):
 class JKOpts(ctypes.Structure):
     _fields_ = [("fp32_cut", ctypes.c_double), ("check_symmetric", ctypes.c_int),
                 ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int), ("profile", ctypes.c_int),
-                ("graph", ctypes.c_int)]
+                ("graph", ctypes.c_int), ("fp32_prim_rel", ctypes.c_double)]
 
 
 class QuartetMeta(ctypes.Structure):

@@ -694,6 +694,7 @@ int run_jk(lai_engine* E, const double* dD, double* dJ, double* dK, cudaStream_t
   args.nbf = nbf;
   args.mode = lai::MODE_JK;
   args.prim_eps = E->prim_eps;
+  args.prim_rel32 = o.fp32_prim_rel;
   if (batched) {
     args.sys_off = E->d_sys_off.as<int64_t>();
     args.sys_nbf = E->d_sys_nbf.as<int>();
@@ -842,6 +843,7 @@ void lai_jk_opts_default(lai_jk_opts* opts) {
   opts->shard_count = 1;
   opts->profile = 0;
   opts->graph = 0;
+  opts->fp32_prim_rel = 0.0;
 }
 
 }  // extern "C"
@@ -983,11 +985,13 @@ int lai_jk_build_device(lai_engine* engine, const double* d_D, double* d_J, doub
   lai_jk_opts_default(&o);
   if (opts) o = *opts;
   if (!(o.fp32_cut >= 0.0)) return fail(LAI_EINVAL, "lai_jk_build_device: fp32_cut must be >= 0");
+  if (!(o.fp32_prim_rel >= 0.0 && o.fp32_prim_rel < 1.0))
+    return fail(LAI_EINVAL, "lai_jk_build_device: fp32_prim_rel must be in [0, 1)");
   LAI_CUDA_TRY(cudaSetDevice(engine->device));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (!o.graph) return run_jk(engine, d_D, d_J, d_K, s, o, report, false);
   if (!s || o.profile) return fail(LAI_EINVAL, "lai_jk_build_device: graph mode needs a stream and profile = 0");
-  lai_engine::GraphKey key{d_D, d_J, d_K, s, o.fp32_cut, o.shard_index, o.shard_count};
+  lai_engine::GraphKey key{d_D, d_J, d_K, s, o.fp32_cut, o.shard_index, o.shard_count, o.fp32_prim_rel};
   if (engine->graph_exec && engine->graph_key == key) {
     LAI_CUDA_TRY(cudaGraphLaunch(engine->graph_exec, s));
     if (report) *report = engine->graph_report;
@@ -1030,6 +1034,8 @@ int lai_jk_build(lai_engine* engine, const double* D, size_t nbf, double* J, dou
   lai_jk_opts_default(&o);
   if (opts) o = *opts;
   if (!(o.fp32_cut >= 0.0)) return fail(LAI_EINVAL, "lai_jk_build: fp32_cut must be >= 0");
+  if (!(o.fp32_prim_rel >= 0.0 && o.fp32_prim_rel < 1.0))
+    return fail(LAI_EINVAL, "lai_jk_build: fp32_prim_rel must be in [0, 1)");
   if (o.check_symmetric) {
     for (size_t i = 0; i < nbf; ++i)
       for (size_t j = 0; j < i; ++j)
@@ -1069,6 +1075,8 @@ int lai_jk_build_batched(lai_engine* engine, const double* D, double* J, double*
   lai_jk_opts_default(&o);
   if (opts) o = *opts;
   if (!(o.fp32_cut >= 0.0)) return fail(LAI_EINVAL, "lai_jk_build_batched: fp32_cut must be >= 0");
+  if (!(o.fp32_prim_rel >= 0.0 && o.fp32_prim_rel < 1.0))
+    return fail(LAI_EINVAL, "lai_jk_build_batched: fp32_prim_rel must be in [0, 1)");
   LAI_CUDA_TRY(cudaSetDevice(engine->device));
   const size_t bytes = sizeof(double) * engine_mat_elems(engine);
   if (engine->d_D.bytes < bytes) {

@@ -168,9 +168,10 @@ struct lai_engine {
     cudaStream_t stream;
     double fp32_cut;
     int shard_index, shard_count;
+    double fp32_prim_rel;
     bool operator==(const GraphKey& o) const {
       return D == o.D && J == o.J && K == o.K && stream == o.stream && fp32_cut == o.fp32_cut &&
-             shard_index == o.shard_index && shard_count == o.shard_count;
+             shard_index == o.shard_index && shard_count == o.shard_count && fp32_prim_rel == o.fp32_prim_rel;
     }
   };
   cudaGraphExec_t graph_exec = nullptr;

@@ -94,6 +94,7 @@ struct JKArgs {
   double* schwarz_out;   // MODE_SCHWARZ: [bra pair] sqrt(max |(ab|ab)|)
   unsigned int* status;  // device status word (0 = ok)
   double prim_eps;       // skip primitive quartets with q_ab * q_cd < prim_eps (0 = none)
+  double prim_rel32;     // FP32 kernels: also skip q_ab * q_cd < prim_rel32 * Q_ij * Q_kl
   unsigned long long* prim_count;  // optional: += primitive quartets executed by the launch
   // batched engines (many independent systems): D, J and K hold one nbf_s x nbf_s
   // block per system, block s at element offset sys_off[s]; function indices are

@@ -68,7 +68,11 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 #pragma unroll
   for (int i = 0; i < NK * NF; ++i) G[i] = R(0);
 
-  const double peps = args.prim_eps;
+  // FP32 quartets (fp32_prim_rel > 0): primitive quartets below that fraction of the
+  // quartet's own Schwarz bound are skipped as well
+  const double peps = (sizeof(R) == 4 && args.prim_rel32 > 0.0)
+                          ? fmax(args.prim_eps, args.prim_rel32 * __ldg(blk.bra.Q + p) * __ldg(blk.ket.Q + q))
+                          : args.prim_eps;
   unsigned int nprim_done = 0;
   for (int ib = 0; ib < Kab; ++ib) {
     // the bra pair's primitive record (BraRecField): the lanes of a quartet group

@@ -285,7 +285,11 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   // primitives (s pairs against p/d pairs) and goes inside, with its next primitive
   // pair loaded one iteration ahead.
   const R* pk0 = kprim + q;
-  const R peps_r = R(peps);
+  // FP32 quartets (fp32_prim_rel > 0): primitive quartets below that fraction of the
+  // quartet's own Schwarz bound are skipped as well
+  const R peps_r = R((F32 && args.prim_rel32 > 0.0)
+                         ? fmax(peps, args.prim_rel32 * __ldg(blk.bra.Q + p) * __ldg(blk.ket.Q + q))
+                         : peps);
   if constexpr (kKetOuter) {
     const R qab_max = ib0 < Kab ? __ldg(bprim + (size_t)ib0 * nbra + p + PF_Q * sb) : R(0);
     KetPrimT<R> nxt;

@@ -174,20 +174,24 @@ class Engine:
         return Q
 
     @staticmethod
-    def _opts(fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False, graph=False):
+    def _opts(fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False, graph=False, fp32_prim_rel=0.0):
         opts = _lib.JKOpts()
         _lib.lib().lai_jk_opts_default(ctypes.byref(opts))
         opts.fp32_cut = fp32_cut
+        opts.fp32_prim_rel = fp32_prim_rel
         opts.check_symmetric = int(check_symmetric)
         opts.shard_index, opts.shard_count = shard
         opts.profile = int(profile)
         opts.graph = int(graph)
         return opts
 
-    def jk(self, D, fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False, out=None):
+    def jk(self, D, fp32_cut=0.0, check_symmetric=False, shard=(0, 1), profile=False, out=None,
+           fp32_prim_rel=0.0):
         """(J, K, report) for a host density D.  ``out`` = (J, K) host arrays to
         fill (e.g. pinned memory); ``shard`` = (index, count) computes one
-        rank's partial J/K of a multi-GPU build."""
+        rank's partial J/K of a multi-GPU build; ``fp32_prim_rel`` skips, in the
+        FP32 quartets only, primitive quartets below that fraction of the
+        quartet's Schwarz bound (lai_jk_opts.fp32_prim_rel)."""
         L = _lib.lib()
         n = self.basis.nbf
         D = np.ascontiguousarray(D, dtype=np.float64)
@@ -198,7 +202,7 @@ class Engine:
             K = np.empty((n, n))
         else:
             J, K = out
-        opts = self._opts(fp32_cut, check_symmetric, shard, profile)
+        opts = self._opts(fp32_cut, check_symmetric, shard, profile, fp32_prim_rel=fp32_prim_rel)
         rep = _lib.JKReport()
         _lib.check(L.lai_jk_build(self._h, D.ctypes.data, n, J.ctypes.data, K.ctypes.data,
                                   ctypes.byref(opts), ctypes.byref(rep)))
@@ -211,11 +215,12 @@ class Engine:
         J, K, rep = self.jk(Dc, fp32_cut=fp32_cut)
         return self.basis.cart_to_sph(J), self.basis.cart_to_sph(K), rep
 
-    def jk_device(self, d_D, d_J, d_K, stream=0, fp32_cut=0.0, shard=(0, 1), profile=False, graph=False):
+    def jk_device(self, d_D, d_J, d_K, stream=0, fp32_cut=0.0, shard=(0, 1), profile=False, graph=False,
+                  fp32_prim_rel=0.0):
         """Device-pointer variant (integers from torch.Tensor.data_ptr()).  graph=True
         captures the build as a CUDA graph on the first call and replays it after."""
         L = _lib.lib()
-        opts = self._opts(fp32_cut, False, shard, profile, graph)
+        opts = self._opts(fp32_cut, False, shard, profile, graph, fp32_prim_rel)
         rep = _lib.JKReport()
         _lib.check(L.lai_jk_build_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
                                          ctypes.c_void_p(d_K), ctypes.c_void_p(stream),

@@ -23,7 +23,7 @@ def test_library_exports_every_declared_symbol(lai):
     for n in names:
         assert hasattr(L, n), n
     assert sorted(lai._lib.EXPORTED) == names
-    assert L.lai_abi_version() == 1
+    assert L.lai_abi_version() == 2
 
 
 def test_basis_normalization_matches_reference(lai):

@@ -244,6 +244,30 @@ def test_mixed_precision_energy_within_bar(lai):
     assert np.max(np.abs(J1 - J1.T)) < 1e-12 and np.max(np.abs(K1 - K1.T)) < 1e-12
 
 
+
+def test_mixed_precision_relative_primitive_cut(lai):
+    """lai_jk_opts.fp32_prim_rel: FP32 quartets also skip primitive quartets below
+    that fraction of their own Schwarz bound.  0 reproduces the plain mixed build
+    (to the run-to-run spread of the FP64 atomic digestion); 1e-6 at cut 1e-6 stays
+    inside the 1e-8 Eh bar and skips nothing in the FP64 quartets; values outside
+    [0, 1) are refused."""
+    w = lai.workloads.make("h2o8_ccpvdz")
+    e = _engine(lai, w.basis)
+    J64, K64, _ = e.jk(w.D)
+    Jm, Km, rm = e.jk(w.D, fp32_cut=1e-6)
+    J0, K0, r0 = e.jk(w.D, fp32_cut=1e-6, fp32_prim_rel=0.0)
+    assert np.max(np.abs(Jm - J0)) < 1e-12 and np.max(np.abs(Km - K0)) < 1e-12
+    Jr, Kr, rr = e.jk(w.D, fp32_cut=1e-6, fp32_prim_rel=1e-6)
+    assert rr.quartets_fp32 == rm.quartets_fp32 > 0
+    dE = 0.5 * np.sum(w.D * (Jr - J64)) - 0.25 * np.sum(w.D * (Kr - K64))
+    assert abs(dE) < 1e-8
+    assert np.max(np.abs(Jr - J64)) < 1e-8 and np.max(np.abs(Kr - K64)) < 1e-8
+    # the FP64 quartets are untouched: with every quartet in FP64 the option is inert
+    Jf, Kf, _ = e.jk(w.D, fp32_cut=0.0, fp32_prim_rel=1e-3)
+    assert np.max(np.abs(Jf - J64)) < 1e-12 and np.max(np.abs(Kf - K64)) < 1e-12
+    with pytest.raises(lai.LibAccIntError):
+        e.jk(w.D, fp32_cut=1e-6, fp32_prim_rel=1.5)
+
 def test_mixed_precision_cut_zero_is_fp64(lai):
     """fp32_cut = 0 is the plain FP64 build (equal up to the order of the FP64
     atomic additions); a negative cut is an error."""
