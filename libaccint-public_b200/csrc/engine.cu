@@ -334,11 +334,18 @@ int launch_block(lai_engine* E, const lai::QuartetBlock& blk, const lai::JKArgs&
   }
   // the other classes: warp-per-quartet, bra-sliced or tiled kernel, as tuned for
   // this block (lai_engine_autotune) or by the measured per-class default; FP32
-  // requests go to the sliced kernel where it exists (the others are FP64 only)
+  // requests go to the sliced kernel where it exists, else to the warp-per-quartet
+  // kernel's FP32 variant (d and f classes; the tiled and generic kernels are FP64
+  // only)
   int kern = tune.kernel != lai::KERNEL_DEFAULT ? tune.kernel : lai::default_kernel(la, lb, lc, ld);
   if (fp32 && lai::sliced_class_supported(la, lb, lc, ld)) kern = lai::KERNEL_SLICED;
+  else if (fp32 && lai::warpq_class_supported(la, lb, lc, ld)) kern = lai::KERNEL_WARPQ;
   if (kern == lai::KERNEL_WARPQ) {
-    const int rc = lai::launch_warpq(blk, args, E->tab, E->stream, E->num_sms);
+    const int rc = lai::launch_warpq(blk, args, E->tab, E->stream, E->num_sms, fp32);
+    if (rc == 1) {
+      if (ran_fp32) *ran_fp32 = true;
+      return LAI_OK;
+    }
     if (rc == 0) return LAI_OK;
     if (rc < -1) return fail(LAI_ECUDA, std::string("warp-per-quartet launch failed: ") +
                                             cudaGetErrorString(lai::warpq_launch_error()));

@@ -32,10 +32,11 @@ bool sliced_class_supported(int la, int lb, int lc, int ld);
 // Warp-per-quartet kernel with lanes over the output integrals (eri_tiled.cu),
 // any class with l <= 4; 0 on success, -1 if the class does not fit shared memory.
 // Warp-per-quartet kernel compile-time specialised per class (J/K mode only).
-// Returns 0 when launched, -1 when the class is not instantiated (or the mode is
-// not J/K), < -1 on a CUDA error.
+// Returns 0 when launched in FP64, 1 when fp32 asked for and got the FP32 variant
+// (d and f classes), -1 when the class is not instantiated (or the mode is not
+// J/K), < -1 on a CUDA error.
 int launch_warpq(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                 int num_sms);
+                 int num_sms, bool fp32 = false);
 cudaError_t warpq_launch_error();  // CUDA error of the last failed launch_warpq
 bool warpq_class_supported(int la, int lb, int lc, int ld);
 // Kernel family of a class outside the thread-per-quartet set when no tuned choice

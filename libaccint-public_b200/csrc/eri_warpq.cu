@@ -17,21 +17,21 @@ namespace lai {
   W(4, 3, 1, 0) W(4, 4, 0, 0) W(4, 4, 1, 0)
 
 int launch_warpq_d(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms);
+                    int num_sms, bool fp32);
 int launch_warpq_f0(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms);
+                    int num_sms, bool fp32);
 int launch_warpq_f1(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms);
+                    int num_sms, bool fp32);
 int launch_warpq_f2(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms);
+                    int num_sms, bool fp32);
 int launch_warpq_g0(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms);
+                    int num_sms, bool fp32);
 int launch_warpq_g1(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms);
+                    int num_sms, bool fp32);
 int launch_warpq_g2(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms);
+                    int num_sms, bool fp32);
 int launch_warpq_g3(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms);
+                    int num_sms, bool fp32);
 
 bool warpq_supported_d(int la, int lb, int lc, int ld);
 bool warpq_supported_f0(int la, int lb, int lc, int ld);
@@ -45,18 +45,18 @@ bool warpq_supported_g3(int la, int lb, int lc, int ld);
 cudaError_t warpq_launch_error() { return warpq_last_error(); }
 
 int launch_warpq(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                 int num_sms) {
+                 int num_sms, bool fp32) {
   if (args.mode != MODE_JK) return -1;
   if (blk.total - blk.t_begin <= 0) return 0;
   int rc;
-  if ((rc = launch_warpq_d(blk, args, tab, stream, num_sms)) != -1) return rc;
-  if ((rc = launch_warpq_f0(blk, args, tab, stream, num_sms)) != -1) return rc;
-  if ((rc = launch_warpq_f1(blk, args, tab, stream, num_sms)) != -1) return rc;
-  if ((rc = launch_warpq_f2(blk, args, tab, stream, num_sms)) != -1) return rc;
-  if ((rc = launch_warpq_g0(blk, args, tab, stream, num_sms)) != -1) return rc;
-  if ((rc = launch_warpq_g1(blk, args, tab, stream, num_sms)) != -1) return rc;
-  if ((rc = launch_warpq_g2(blk, args, tab, stream, num_sms)) != -1) return rc;
-  if ((rc = launch_warpq_g3(blk, args, tab, stream, num_sms)) != -1) return rc;
+  if ((rc = launch_warpq_d(blk, args, tab, stream, num_sms, fp32)) != -1) return rc;
+  if ((rc = launch_warpq_f0(blk, args, tab, stream, num_sms, fp32)) != -1) return rc;
+  if ((rc = launch_warpq_f1(blk, args, tab, stream, num_sms, fp32)) != -1) return rc;
+  if ((rc = launch_warpq_f2(blk, args, tab, stream, num_sms, fp32)) != -1) return rc;
+  if ((rc = launch_warpq_g0(blk, args, tab, stream, num_sms, fp32)) != -1) return rc;
+  if ((rc = launch_warpq_g1(blk, args, tab, stream, num_sms, fp32)) != -1) return rc;
+  if ((rc = launch_warpq_g2(blk, args, tab, stream, num_sms, fp32)) != -1) return rc;
+  if ((rc = launch_warpq_g3(blk, args, tab, stream, num_sms, fp32)) != -1) return rc;
   return -1;
 }
 

@@ -10,10 +10,10 @@ namespace lai {
   X(3, 0, 3, 0) X(3, 1, 1, 0) X(3, 1, 1, 1) X(3, 1, 2, 0)
 
 int launch_warpq_f0(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab, cudaStream_t stream,
-                    int num_sms) {
+                    int num_sms, bool fp32) {
   const int la = blk.bra.la, lb = blk.bra.lb, lc = blk.ket.la, ld = blk.ket.lb;
 #define X(a, b, c, d) \
-  if (la == a && lb == b && lc == c && ld == d) return launch_warpq_cls<a, b, c, d>(blk, args, tab, stream, num_sms);
+  if (la == a && lb == b && lc == c && ld == d) return launch_warpq_cls<a, b, c, d, true>(blk, args, tab, stream, num_sms, fp32);
   LAI_WARPQ_CLASSES(X)
 #undef X
   return -1;

@@ -100,7 +100,12 @@ __device__ __forceinline__ double warpq_pow(double x, int m) {
   return r;
 }
 
-template <int LA, int LB, int LC, int LD>
+// R = double: the whole quartet in FP64.  R = float (the FP32 part of a mixed
+// build, d and f classes): roots, 2D tables and the (e0|f0) accumulation in FP32
+// (the tables take half the shared memory and its bandwidth); the primitive-pair
+// quantities up to T and the prefactor, the transfer, normalization and digestion
+// stay FP64.
+template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>::MIN_BLOCKS)) eri_warpq_kernel(QuartetBlock blk, JKArgs args,
                                                                      RysTablesView tab) {
   using C = WarpqClass<LA, LB, LC, LD>;
@@ -200,7 +205,8 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
       const int ce = cart_comp(le, re), cf = cart_comp(lf, rf);
       const int ox = comp_x(ce) * W + comp_x(cf), oy = comp_y(ce) * W + comp_y(cf),
                 oz = comp_z(ce) * W + comp_z(cf);
-      o = (ox * 8) | ((oy * 8) << 10) | ((oz * 8) << 20);
+      constexpr int sz = sizeof(R);
+      o = (ox * sz) | ((oy * sz) << 10) | ((oz * sz) << 20);
     }
     goff[m] = o;
   }
@@ -262,9 +268,9 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
       Ds[i] = __ldg(mats.D + (size_t)(r0 + k / c1) * n + c0 + k % c1);
     }
 
-    double G[MG];
+    R G[MG];
 #pragma unroll
-    for (int m = 0; m < MG; ++m) G[m] = 0.0;
+    for (int m = 0; m < MG; ++m) G[m] = R(0);
 
     // the whole warp works on one quartet: bra and ket primitives come from their
     // per-pair records (a few contiguous lines per pair, 16-byte loads)
@@ -296,26 +302,27 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
         const double pref = cab * ccd * rs;
         if (lane < 3 * NR) {
           const int r = lane / 3, x = lane - 3 * r;
-          double u, w;
-          rys_root_one<double>(NR, r, T, tab, u, w);
-          const double pqx = x == 0 ? PQx : x == 1 ? PQy : PQz;
-          const double pax = x == 0 ? PAx : x == 1 ? PAy : PAz;
-          const double qcx = __ldg(pkr + BR_PAX + x);
-          const double pa = pax - rz * u * pqx;
-          const double qc = qcx + re * u * pqx;
-          const double b00 = 0.5 * inv * u, b10 = hz - hz * rz * u, b01 = he - he * re * u;
-          double V[LAB + 1][W];
-          V[0][0] = (x == 2) ? w * pref : 1.0;
+          R u, w;
+          rys_root_one<R>(NR, r, R(T), tab, u, w);
+          const R pqx = R(x == 0 ? PQx : x == 1 ? PQy : PQz);
+          const R pax = R(x == 0 ? PAx : x == 1 ? PAy : PAz);
+          const R qcx = R(__ldg(pkr + BR_PAX + x));
+          const R rzr = R(rz), rer = R(re);
+          const R pa = pax - rzr * u * pqx;
+          const R qc = qcx + rer * u * pqx;
+          const R b00 = R(0.5) * R(inv) * u, b10 = R(hz) - R(hz) * rzr * u, b01 = R(he) - R(he) * rer * u;
+          R V[LAB + 1][W];
+          V[0][0] = (x == 2) ? w * R(pref) : R(1);
 #pragma unroll
           for (int e = 0; e < LAB; ++e)
-            V[e + 1][0] = pa * V[e][0] + (e ? double(e) * b10 * V[e > 0 ? e - 1 : 0][0] : 0.0);
+            V[e + 1][0] = pa * V[e][0] + (e ? R(e) * b10 * V[e > 0 ? e - 1 : 0][0] : R(0));
 #pragma unroll
           for (int f = 0; f < LCD; ++f)
 #pragma unroll
             for (int e = 0; e <= LAB; ++e)
-              V[e][f + 1] = qc * V[e][f] + (f ? double(f) * b01 * V[e][f > 0 ? f - 1 : 0] : 0.0) +
-                            (e ? double(e) * b00 * V[e > 0 ? e - 1 : 0][f] : 0.0);
-          double* dst = Vs + (r * 3 + x) * VS;
+              V[e][f + 1] = qc * V[e][f] + (f ? R(f) * b01 * V[e][f > 0 ? f - 1 : 0] : R(0)) +
+                            (e ? R(e) * b00 * V[e > 0 ? e - 1 : 0][f] : R(0));
+          R* dst = reinterpret_cast<R*>(Vs) + (r * 3 + x) * VS;
 #pragma unroll
           for (int e = 0; e <= LAB; ++e)
 #pragma unroll
@@ -324,15 +331,15 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
         __syncwarp();
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-          const char* vx = reinterpret_cast<const char*>(Vs + (r * 3) * VS);
-          const char* vy = vx + VS * 8;
-          const char* vz = vy + VS * 8;
+          const char* vx = reinterpret_cast<const char*>(reinterpret_cast<const R*>(Vs) + (r * 3) * VS);
+          const char* vy = vx + VS * sizeof(R);
+          const char* vz = vy + VS * sizeof(R);
 #pragma unroll
           for (int m = 0; m < MG; ++m) {
             const int o = goff[m];
-            G[m] += *reinterpret_cast<const double*>(vx + (o & 1023)) *
-                    *reinterpret_cast<const double*>(vy + ((o >> 10) & 1023)) *
-                    *reinterpret_cast<const double*>(vz + (o >> 20));
+            G[m] += *reinterpret_cast<const R*>(vx + (o & 1023)) *
+                    *reinterpret_cast<const R*>(vy + ((o >> 10) & 1023)) *
+                    *reinterpret_cast<const R*>(vz + (o >> 20));
           }
         }
         __syncwarp();
@@ -343,7 +350,7 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
 #pragma unroll
     for (int m = 0; m < MG; ++m) {
       const int j = lane + 32 * m;
-      if (j < C::NG) B0[j] = G[m];
+      if (j < C::NG) B0[j] = double(G[m]);
     }
     const double ABx = __ldg(blk.bra.AB + p), ABy = __ldg(blk.bra.AB + nbra + p),
                  ABz = __ldg(blk.bra.AB + 2 * nbra + p);
@@ -457,19 +464,19 @@ __global__ void __launch_bounds__(kWarpqWarps * 32, (WarpqClass<LA, LB, LC, LD>:
 
 // Host side: per-warp shared memory of class (la, lb, lc, ld), or -1 when the
 // class is not instantiated.
-template <int LA, int LB, int LC, int LD>
-int launch_warpq_cls(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
-                     cudaStream_t stream, int num_sms) {
+template <int LA, int LB, int LC, int LD, typename R>
+int launch_warpq_typed(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
+                       cudaStream_t stream, int num_sms) {
   using C = WarpqClass<LA, LB, LC, LD>;
   const size_t smem = (size_t)C::PER_WARP * 8 * kWarpqWarps;
   static int per_sm = -1;
   if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(eri_warpq_kernel<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(eri_warpq_kernel<LA, LB, LC, LD, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return -3;
   if (per_sm < 0) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, eri_warpq_kernel<LA, LB, LC, LD>, kWarpqWarps * 32,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, eri_warpq_kernel<LA, LB, LC, LD, R>, kWarpqWarps * 32,
                                                       smem) != cudaSuccess)
       return -3;
     if (b <= 0) return -1;  // does not fit: the tiled kernel takes the class
@@ -478,13 +485,27 @@ int launch_warpq_cls(const QuartetBlock& blk, const JKArgs& args, const RysTable
   const int64_t want = (blk.total - blk.t_begin + kWarpqWarps - 1) / kWarpqWarps;
   const int64_t cap = (int64_t)num_sms * per_sm;
   const int grid = (int)std::min<int64_t>(want, cap);
-  eri_warpq_kernel<LA, LB, LC, LD><<<grid, kWarpqWarps * 32, smem, stream>>>(blk, args, tab);
+  eri_warpq_kernel<LA, LB, LC, LD, R><<<grid, kWarpqWarps * 32, smem, stream>>>(blk, args, tab);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     warpq_last_error() = e;
     return -3;
   }
   return 0;
+}
+
+// FP32 = the units instantiating an FP32 variant (d and f classes); fp32 asks for
+// it (returns 1 when the FP32 kernel ran, 0 for FP64, <0 as launch_warpq).
+template <int LA, int LB, int LC, int LD, bool FP32>
+int launch_warpq_cls(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
+                     cudaStream_t stream, int num_sms, bool fp32) {
+  if constexpr (FP32) {
+    if (fp32) {
+      const int rc = launch_warpq_typed<LA, LB, LC, LD, float>(blk, args, tab, stream, num_sms);
+      return rc == 0 ? 1 : rc;
+    }
+  }
+  return launch_warpq_typed<LA, LB, LC, LD, double>(blk, args, tab, stream, num_sms);
 }
 
 }  // namespace lai

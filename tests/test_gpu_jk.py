@@ -268,6 +268,36 @@ def test_mixed_precision_relative_primitive_cut(lai):
     with pytest.raises(lai.LibAccIntError):
         e.jk(w.D, fp32_cut=1e-6, fp32_prim_rel=1.5)
 
+
+def test_mixed_precision_f_classes_run_fp32(lai):
+    """(H2O)2 / cc-pVTZ (f on O) at cut 1e-6: quartets of f classes below the FP32
+    Schwarz cut run in FP32 (the warp-per-quartet FP32 variant; only classes too
+    large for it stay FP64): the FP32 count, checked against the canonical
+    quartets in [threshold, cut) worked out on the host from the engine's Schwarz
+    matrix, exceeds what the classes up to d hold, and the energy stays inside the
+    1e-8 Eh bar."""
+    w = lai.workloads.make("h2o2_ccpvtz")
+    e = _engine(lai, w.basis)
+    Q = e.schwarz()
+    ls = np.array([s.l for s in w.basis.shells])
+    n = len(ls)
+    i, j = np.tril_indices(n)
+    q = Q[i, j]
+    J64, K64, r64 = e.jk(w.D)
+    Jm, Km, rm = e.jk(w.D, fp32_cut=1e-6)
+    cut = rm.fp32_schwarz_cut
+    assert cut > 0
+    prod = np.multiply.outer(q, q)[np.tril_indices(len(q))]  # canonical pairs of pairs
+    lmax = np.maximum.outer(np.maximum(ls[i], ls[j]), np.maximum(ls[i], ls[j]))[np.tril_indices(len(q))]
+    keep = prod >= 1e-12
+    assert int(keep.sum()) == r64.quartets_fp64
+    below = keep & (prod < cut)
+    assert int((below & (lmax == 3)).sum()) > 0
+    assert int((below & (lmax <= 2)).sum()) < rm.quartets_fp32 <= int(below.sum())
+    dE = 0.5 * np.sum(w.D * (Jm - J64)) - 0.25 * np.sum(w.D * (Km - K64))
+    assert abs(dE) < 1e-8
+    assert np.max(np.abs(Jm - J64)) < 1e-8 and np.max(np.abs(Km - K64)) < 1e-8
+
 def test_mixed_precision_cut_zero_is_fp64(lai):
     """fp32_cut = 0 is the plain FP64 build (equal up to the order of the FP64
     atomic additions); a negative cut is an error."""
