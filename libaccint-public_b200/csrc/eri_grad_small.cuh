@@ -10,9 +10,10 @@
 // (kappa = alpha, beta or gamma, the exponent on the derivative centre), and the
 // horizontal transfer (closed binomial form, the exact A-B and C-D) and the
 // contraction with G_abcd = s n_a n_b n_c n_d (4 D_ab D_cd - D_ac D_bd - D_ad D_bc)
-// run once per contracted quartet.  One launch per centre (DER = A, B or C) keeps
-// the live accumulators to one W and one U block; each launch adds its centre's
-// derivative and subtracts it from the D centre.
+// run once per contracted quartet.  Each pass adds its centres' derivatives and
+// subtracts them from the D centre; how many passes a class takes depends on how
+// many accumulators fit in registers: all three centres in one pass (the
+// smallest classes), A and B in one pass and C in a second, or one per centre.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -26,7 +27,7 @@
 namespace lai {
 namespace grad_small {
 
-enum { DA = 0, DB = 1, DC = 2, DAB = 3 };  // DAB: the A and B centres in one pass
+enum { DA = 0, DB = 1, DC = 2, DAB = 3, DABC = 4 };  // DAB: A and B in one pass; DABC: all three
 
 template <int B, int E, typename F>
 __device__ __forceinline__ void gfor(F&& f) {
@@ -84,19 +85,25 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   // raised block W (W2: the B block of a merged A+B pass) and lowered block U, as
   // shell ranges [E0, E1] x [F0, F1]
-  constexpr bool AB_ = DER == DAB;
+  // ABC_: all three centres in one pass (W: A, W2: B, W3: C); AB_: A and B
+  constexpr bool ABC_ = DER == DABC;
+  constexpr bool AB_ = DER == DAB || ABC_;
   constexpr int WE0 = (DER == DA || AB_) ? LA + 1 : LA, WE1 = DER == DC ? LAB : LAB + 1;
   constexpr int WF0 = DER == DC ? LC + 1 : LC, WF1 = DER == DC ? LCD + 1 : LCD;
-  constexpr bool HAS_U = DER == DA ? LA >= 1 : DER == DB ? LB >= 1 : DER == DC ? LC >= 1 : (LA >= 1 || LB >= 1);
+  constexpr bool HAS_U = DER == DA ? LA >= 1 : DER == DB ? LB >= 1 : DER == DC ? LC >= 1
+                         : DER == DAB ? (LA >= 1 || LB >= 1) : (LA >= 1 || LB >= 1 || LC >= 1);
+  // the lowered block: one rectangle covering the lowered ranges of the pass's centres
   constexpr int UE0 = (DER == DA || AB_) ? (LA >= 1 ? LA - 1 : 0) : LA;
-  constexpr int UE1 = DER == DC ? LAB : LAB - 1;
-  constexpr int UF0 = DER == DC ? (LC >= 1 ? LC - 1 : 0) : LC;
+  constexpr int UE1 = (DER == DC || (ABC_ && LC >= 1)) ? LAB : LAB - 1;
+  constexpr int UF0 = (DER == DC || ABC_) ? (LC >= 1 ? LC - 1 : 0) : LC;
   constexpr int UF1 = DER == DC ? LCD - 1 : LCD;
   constexpr int NWE = ncart_range(WE0, WE1), NWF = ncart_range(WF0, WF1);
   constexpr int NW2E = AB_ ? ncart_range(LA, LAB + 1) : 1;  // W2: e in [LA, LAB+1], f as W
+  constexpr int NW3E = ABC_ ? ncart_range(LA, LAB) : 1;     // W3: e in [LA, LAB], f in [LC+1, LCD+1]
+  constexpr int NW3F = ABC_ ? ncart_range(LC + 1, LCD + 1) : 1;
   constexpr int NUE = HAS_U ? ncart_range(UE0, UE1) : 1, NUF = HAS_U ? ncart_range(UF0, UF1) : 1;
   constexpr int EM = DER == DC ? LAB : LAB + 1;  // vertical recurrence extents
-  constexpr int FM = DER == DC ? LCD + 1 : LCD;
+  constexpr int FM = (DER == DC || ABC_) ? LCD + 1 : LCD;
 
   // the Boys grid / the Rys fit table of NR roots, staged once per block (per-lane
   // gathers from global memory would touch up to 32 lines per load)
@@ -124,7 +131,9 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
     int p = pw;
     while (t >= __ldg(blk.offsets + p + 1)) ++p;
     const int q = (blk.qbegin ? __ldg(blk.qbegin + p) : 0) + (int)(t - __ldg(blk.offsets + p));
-    double W[NWE * NWF], W2[AB_ ? NW2E * NWF : 1], U[NUE * NUF];
+    double W[NWE * NWF], W2[AB_ ? NW2E * NWF : 1], W3[NW3E * NW3F], U[NUE * NUF];
+#pragma unroll
+    for (int i = 0; i < NW3E * NW3F; ++i) W3[i] = 0.0;
 #pragma unroll
     for (int i = 0; i < NWE * NWF; ++i) W[i] = 0.0;
 #pragma unroll
@@ -149,7 +158,7 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
         const double qcd = __ldg(pk + PF_Q * sk);
         if (qab * qcd < ga.prim_eps) break;
         const double eta = __ldg(pk + PF_ZETA * sk), he = __ldg(pk + PF_HZ * sk);
-        const double gamma = DER == DC ? __ldg(pk + PF_ALPHA * sk) : 0.0;
+        const double gamma = (DER == DC || ABC_) ? __ldg(pk + PF_ALPHA * sk) : 0.0;
         const double PQ[3] = {P[0] - __ldg(pk + PF_PX * sk), P[1] - __ldg(pk + PF_PY * sk),
                               P[2] - __ldg(pk + PF_PZ * sk)};
         const double QC[3] = {__ldg(pk + PF_PAX * sk), __ldg(pk + PF_PAY * sk), __ldg(pk + PF_PAZ * sk)};
@@ -161,6 +170,7 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
         const double pref = cab * ccd * rs;
         const double kap2 = 2.0 * ((DER == DA || AB_) ? alpha : DER == DB ? zeta - alpha : gamma);
         const double kapb2 = 2.0 * (zeta - alpha);  // the B block of a merged pass
+        const double kapc2 = 2.0 * gamma;           // the C block of an all-centre pass
         double u[NR], w[NR];
         rys_smem<NR, double>(T, stab, tab, u, w);
 #pragma unroll
@@ -182,6 +192,20 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
               for (int e = 0; e <= EM; ++e)
                 I[x][e][f + 1] = qc * I[x][e][f] + (f ? f * b01 * I[x][e][f > 0 ? f - 1 : 0] : 0.0) +
                                  (e ? e * b00 * I[x][e > 0 ? e - 1 : 0][f] : 0.0);
+          }
+          if constexpr (ABC_) {
+            gfor<0, NW3E>([&](auto IE) {
+              constexpr int ie = decltype(IE)::value;
+              constexpr int le = [] { int l = LA, r = ie; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
+              constexpr int ce = cart_comp(le, ie - ncart_before(LA, le));
+              gfor<0, NW3F>([&](auto JF) {
+                constexpr int jf = decltype(JF)::value;
+                constexpr int lf = [] { int l = LC + 1, r = jf; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
+                constexpr int cf = cart_comp(lf, jf - ncart_before(LC + 1, lf));
+                W3[ie * NW3F + jf] += kapc2 * I[0][comp_x(ce)][comp_x(cf)] * I[1][comp_y(ce)][comp_y(cf)] *
+                                      I[2][comp_z(ce)][comp_z(cf)];
+              });
+            });
           }
           if constexpr (AB_) {
             // merged A+B pass: the products over e in [LA, LAB+1] once, into the B
@@ -255,6 +279,7 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
     const double* __restrict__ D = ga.D;
     const size_t nbf = (size_t)ga.nbf;
     double g[3] = {0.0, 0.0, 0.0}, g2[3] = {0.0, 0.0, 0.0};  // g2: the B centre of a merged pass
+    double g3[3] = {0.0, 0.0, 0.0};                         // g3: the C centre of an all-centre pass
     constexpr int D1 = AB_ ? DA : DER;  // the centre g belongs to
     gfor<0, NA>([&](auto IA) {
       constexpr int a = decltype(IA)::value;
@@ -324,6 +349,25 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
                 }
                 g2[x] += G * accb;
               }
+              if constexpr (ABC_) {  // the C centre: W3 over f in [LC+1, LCD+1], U for c - 1x
+                double accc = 0.0;
+                hrr_terms<ca, cb, LA>(abp, [&](auto E, double hb) {
+                  hrr_terms<shift(cc, x, 1), cd, LC + 1>(cdp, [&](auto F, double hd) {
+                    accc += hb * hd * W3[decltype(E)::value * NW3F + decltype(F)::value];
+                  });
+                });
+                constexpr int ncx = comp_n(cc, x);
+                if constexpr (HAS_U && ncx > 0) {
+                  double low = 0.0;
+                  hrr_terms<ca, cb, UE0>(abp, [&](auto E, double hb) {
+                    hrr_terms<shift(cc, x, -1), cd, UF0>(cdp, [&](auto F, double hd) {
+                      low += hb * hd * U[decltype(E)::value * NUF + decltype(F)::value];
+                    });
+                  });
+                  accc -= ncx * low;
+                }
+                g3[x] += G * accc;
+              }
             });
           });
         });
@@ -336,12 +380,17 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
       atomicAdd(ga.grad + 3 * at + x, g[x]);
-      atomicAdd(ga.grad + 3 * atD + x, -(g[x] + g2[x]));
+      atomicAdd(ga.grad + 3 * atD + x, -(g[x] + g2[x] + g3[x]));
     }
     if constexpr (AB_) {
       const int atB = __ldg(ga.shell_atom + __ldg(blk.bra.shell_b + p));
 #pragma unroll
       for (int x = 0; x < 3; ++x) atomicAdd(ga.grad + 3 * atB + x, g2[x]);
+    }
+    if constexpr (ABC_) {
+      const int atC = __ldg(ga.shell_atom + __ldg(blk.ket.shell_a + q));
+#pragma unroll
+      for (int x = 0; x < 3; ++x) atomicAdd(ga.grad + 3 * atC + x, g3[x]);
     }
   }
 }
@@ -357,31 +406,44 @@ int launch(const QuartetBlock& blk, const GradSmallArgs& ga, const RysTablesView
   constexpr int nf = ncart_range(LC, LCD);
   constexpr int merged_size = (ncart_range(LA + 1, LAB + 1) + ncart_range(LA, LAB + 1) +
                                ((LA >= 1 || LB >= 1) ? ncart_range(LA >= 1 ? LA - 1 : 0, LAB - 1) : 0)) * nf;
-  constexpr bool kMerge = merged_size <= 40;
+  constexpr bool kMerge = merged_size <= 48;
+  // all three centres in one pass when that pass's blocks stay small too
+  constexpr int all_size = merged_size + ncart_range(LA, LAB) * ncart_range(LC + 1, LCD + 1) +
+                           ((LC >= 1) ? ncart_range(LA, LAB) * ncart(LC - 1) : 0);
+  constexpr bool kAll = all_size <= 72;
   const size_t smem = table_bytes<NR, double>();
+  // only the kernels this class launches are instantiated (and given their shared memory)
+  auto allow = [&](auto kern) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
+  };
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(grad_small_kernel<LA, LB, LC, LD, DA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(grad_small_kernel<LA, LB, LC, LD, DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(grad_small_kernel<LA, LB, LC, LD, DC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess ||
-        (kMerge && cudaFuncSetAttribute(grad_small_kernel<LA, LB, LC, LD, DAB>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess))
-      return -3;
+    bool ok;
+    if constexpr (kAll) {
+      ok = allow(grad_small_kernel<LA, LB, LC, LD, DABC>);
+    } else if constexpr (kMerge) {
+      ok = allow(grad_small_kernel<LA, LB, LC, LD, DAB>) && allow(grad_small_kernel<LA, LB, LC, LD, DC>);
+    } else {
+      ok = allow(grad_small_kernel<LA, LB, LC, LD, DA>) && allow(grad_small_kernel<LA, LB, LC, LD, DB>) &&
+           allow(grad_small_kernel<LA, LB, LC, LD, DC>);
+    }
+    if (!ok) return -3;
     attr = true;
   }
   const int threads = 128;
   const int64_t want = (nq + threads - 1) / threads;
   const int grid = (int)(want < (int64_t)num_sms * 8 ? want : (int64_t)num_sms * 8);
-  if constexpr (kMerge) {
-    grad_small_kernel<LA, LB, LC, LD, DAB><<<grid, threads, smem, stream>>>(blk, ga, tab);
+  if constexpr (kAll) {
+    grad_small_kernel<LA, LB, LC, LD, DABC><<<grid, threads, smem, stream>>>(blk, ga, tab);
   } else {
-    grad_small_kernel<LA, LB, LC, LD, DA><<<grid, threads, smem, stream>>>(blk, ga, tab);
-    grad_small_kernel<LA, LB, LC, LD, DB><<<grid, threads, smem, stream>>>(blk, ga, tab);
+    if constexpr (kMerge) {
+      grad_small_kernel<LA, LB, LC, LD, DAB><<<grid, threads, smem, stream>>>(blk, ga, tab);
+    } else {
+      grad_small_kernel<LA, LB, LC, LD, DA><<<grid, threads, smem, stream>>>(blk, ga, tab);
+      grad_small_kernel<LA, LB, LC, LD, DB><<<grid, threads, smem, stream>>>(blk, ga, tab);
+    }
+    grad_small_kernel<LA, LB, LC, LD, DC><<<grid, threads, smem, stream>>>(blk, ga, tab);
   }
-  grad_small_kernel<LA, LB, LC, LD, DC><<<grid, threads, smem, stream>>>(blk, ga, tab);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 
