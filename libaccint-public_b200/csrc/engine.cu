@@ -308,6 +308,23 @@ int upload_class(PairClassHost& c) {
     LAI_CUDA_TRY(upload(c.d_primb, rb));
     LAI_CUDA_TRY(upload(c.d_primbf, rbf));
   }
+  {  // ket tiles of 32 pairs (lai::KetRecField), FP64 and FP32; pad lanes stay 0
+    const int n = c.n(), Kab = c.Ka * c.Kb;
+    const size_t ntile = ((size_t)n + lai::kKetTile - 1) / lai::kKetTile;
+    std::vector<double> rk(ntile * Kab * lai::kKetRec * lai::kKetTile, 0.0);
+    static const int from[lai::kKetRec] = {lai::PF_Q,   lai::PF_ZETA, lai::PF_HZ,  lai::PF_PX,
+                                           lai::PF_PY,  lai::PF_PZ,   lai::PF_PAX, lai::PF_PAY,
+                                           lai::PF_PAZ, lai::PF_C,    lai::PF_ALPHA};
+    for (int p = 0; p < n; ++p)
+      for (int t = 0; t < Kab; ++t)
+        for (int f = 0; f < lai::kKetRec; ++f)
+          rk[(((size_t)(p / lai::kKetTile) * Kab + t) * lai::kKetRec + f) * lai::kKetTile + p % lai::kKetTile] =
+              c.prim[((size_t)from[f] * Kab + t) * n + p];
+    std::vector<float> rkf(rk.size());
+    for (size_t i = 0; i < rk.size(); ++i) rkf[i] = (float)rk[i];
+    LAI_CUDA_TRY(upload(c.d_primk, rk));
+    LAI_CUDA_TRY(upload(c.d_primkf, rkf));
+  }
   return LAI_OK;
 }
 

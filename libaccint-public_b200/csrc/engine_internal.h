@@ -87,7 +87,8 @@ struct PairClassHost {
   std::vector<double> prim;        // SoA [PF_COUNT][Kab][n]
   int n() const { return (int)sa.size(); }
   // device copies
-  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_Acen, d_prim, d_sys, d_primf, d_primb, d_primbf;
+  DevBuf d_sa, d_sb, d_fa, d_fb, d_Q, d_AB, d_Acen, d_prim, d_sys, d_primf, d_primb, d_primbf, d_primk,
+      d_primkf;
   bool batched = false;             // d_sys is set (more than one system)
   lai::PairClassDev view() const {
     lai::PairClassDev v;
@@ -101,6 +102,8 @@ struct PairClassHost {
     v.primf = d_primf.as<float>();
     v.primb = d_primb.as<double>();
     v.primbf = d_primbf.as<float>();
+    v.primk = d_primk.as<double>();
+    v.primkf = d_primkf.as<float>();
     return v;
   }
 };

@@ -145,6 +145,34 @@ __device__ __forceinline__ void load_ket_prim(const T* __restrict__ pk, size_t s
   k.c = __ldg(pk + PF_C * sk);
 }
 
+// Ket tiles (KetRecField): the address of primitive 0 of pair q, the distance
+// between consecutive primitives of one pair, and one primitive's fields, all at
+// compile-time offsets from that address.
+constexpr int kKetPrimStride = kKetRec * kKetTile;
+template <typename T>
+__device__ __forceinline__ const T* ket_tile_ptr(const T* __restrict__ tiles, int q, int Kcd) {
+  return tiles + (size_t)(q / kKetTile) * Kcd * kKetPrimStride + (q % kKetTile);
+}
+template <typename T>
+__device__ __forceinline__ void load_ket_rec(const T* __restrict__ pk, KetPrimT<T>& k) {
+  k.q = __ldg(pk + KR_Q * kKetTile);
+  k.eta = __ldg(pk + KR_ETA * kKetTile);
+  k.he = __ldg(pk + KR_HE * kKetTile);
+  k.px = __ldg(pk + KR_PX * kKetTile);
+  k.py = __ldg(pk + KR_PY * kKetTile);
+  k.pz = __ldg(pk + KR_PZ * kKetTile);
+  k.qcx = __ldg(pk + KR_QCX * kKetTile);
+  k.qcy = __ldg(pk + KR_QCY * kKetTile);
+  k.qcz = __ldg(pk + KR_QCZ * kKetTile);
+  k.c = __ldg(pk + KR_C * kKetTile);
+}
+template <typename R>
+__device__ __forceinline__ const R* ket_tiles(const PairClassDev& c);
+template <>
+__device__ __forceinline__ const double* ket_tiles<double>(const PairClassDev& c) { return c.primk; }
+template <>
+__device__ __forceinline__ const float* ket_tiles<float>(const PairClassDev& c) { return c.primkf; }
+
 // Primitive-pair table of a class in the kernel's compute type: the FP64 table,
 // or its FP32 copy for the FP32 kernels.
 template <typename R>

@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
   __syncthreads();
   const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
   const int Kab = blk.bra.Ka * blk.bra.Kb, Kcd = blk.ket.Ka * blk.ket.Kb;
-  const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
+  const size_t sb = (size_t)Kab * nbra;
   // warps take chunks of 32 consecutive quartets (grid-stride); one bra search per
   // chunk, then each lane steps forward to its own bra pair (usually the same)
   const int lane = threadIdx.x & 31;
@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
     int p = pw;
     while (t >= __ldg(blk.offsets + p + 1)) ++p;
     const int q = (blk.qbegin ? __ldg(blk.qbegin + p) : 0) + (int)(t - __ldg(blk.offsets + p));
+    const double* __restrict__ pkt = ket_tile_ptr(blk.ket.primk, q, Kcd);
     double W[NWE * NWF], W2[AB_ ? NW2E * NWF : 1], W3[NW3E * NW3F], U[NUE * NUF];
 #pragma unroll
     for (int i = 0; i < NW3E * NW3F; ++i) W3[i] = 0.0;
@@ -154,15 +155,17 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
       const double P[3] = {b2.x, b2.y, b3.x};
       const double PA[3] = {b4.x, b4.y, b5.x};
       for (int ik = 0; ik < Kcd; ++ik) {
-        const double* pk = blk.ket.prim + (size_t)ik * nket + q;
-        const double qcd = __ldg(pk + PF_Q * sk);
+        // ket primitive ik of pair q in the ket tiles (fields at fixed offsets)
+        const double* pk = pkt + (size_t)ik * kKetPrimStride;
+        const double qcd = __ldg(pk + KR_Q * kKetTile);
         if (qab * qcd < ga.prim_eps) break;
-        const double eta = __ldg(pk + PF_ZETA * sk), he = __ldg(pk + PF_HZ * sk);
-        const double gamma = (DER == DC || ABC_) ? __ldg(pk + PF_ALPHA * sk) : 0.0;
-        const double PQ[3] = {P[0] - __ldg(pk + PF_PX * sk), P[1] - __ldg(pk + PF_PY * sk),
-                              P[2] - __ldg(pk + PF_PZ * sk)};
-        const double QC[3] = {__ldg(pk + PF_PAX * sk), __ldg(pk + PF_PAY * sk), __ldg(pk + PF_PAZ * sk)};
-        const double ccd = __ldg(pk + PF_C * sk);
+        const double eta = __ldg(pk + KR_ETA * kKetTile), he = __ldg(pk + KR_HE * kKetTile);
+        const double gamma = (DER == DC || ABC_) ? __ldg(pk + KR_ALPHA * kKetTile) : 0.0;
+        const double PQ[3] = {P[0] - __ldg(pk + KR_PX * kKetTile), P[1] - __ldg(pk + KR_PY * kKetTile),
+                              P[2] - __ldg(pk + KR_PZ * kKetTile)};
+        const double QC[3] = {__ldg(pk + KR_QCX * kKetTile), __ldg(pk + KR_QCY * kKetTile),
+                              __ldg(pk + KR_QCZ * kKetTile)};
+        const double ccd = __ldg(pk + KR_C * kKetTile);
         const double rs = rsqrt(zeta + eta);
         const double inv = rs * rs;
         const double rz = eta * inv, re = zeta * inv;

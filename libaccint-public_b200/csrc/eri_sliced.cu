@@ -61,7 +61,6 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 
   const int Kab = blk.bra.Ka * blk.bra.Kb;
   const int Kcd = blk.ket.Ka * blk.ket.Kb;
-  const size_t sk = (size_t)Kcd * nket;
   (void)nbra;
 
   R G[NK * NF];
@@ -90,13 +89,13 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
     const double Px = b2.x, Py = b2.y, Pz = b3.x;
     const R PAx = R(b4.x), PAy = R(b4.y), PAz = R(b5.x);
     const R cab = R(b1.y);
-    const double* pk0 = blk.ket.prim + q;
+    const double* pkt = ket_tile_ptr(blk.ket.primk, q, Kcd);
     KetPrim nxt;
-    load_ket_prim(pk0, sk, nxt);
+    load_ket_rec(pkt, nxt);
     for (int ik = 0; ik < Kcd; ++ik) {
       const KetPrim cur = nxt;
       if (qab * cur.q < peps) break;  // sorted: the rest are smaller
-      if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
+      if (ik + 1 < Kcd) load_ket_rec(pkt + (size_t)(ik + 1) * kKetPrimStride, nxt);
       ++nprim_done;
       const R eta = R(cur.eta);
       const R he = R(cur.he);

@@ -85,7 +85,7 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
 
   const int Kab = blk.bra.Ka * blk.bra.Kb;
   const int Kcd = blk.ket.Ka * blk.ket.Kb;
-  const size_t sb = (size_t)Kab * nbra, sk = (size_t)Kcd * nket;
+  const size_t sb = (size_t)Kab * nbra;
 
   constexpr bool F32 = sizeof(R) == 4;
   // FP32: the primitive terms of one inner loop are summed in G, which is then
@@ -126,7 +126,6 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   // primitive pair `cur`; accumulates into G.  The FP32 kernels read an FP32 copy
   // of the pair tables (half the bytes and registers, no conversions).
   const R* __restrict__ bprim = prim_table<R>(blk.bra);
-  const R* __restrict__ kprim = prim_table<R>(blk.ket);
   struct BraVals {
     R zeta, hz, Px, Py, Pz, PAx, PAy, PAz, cab;
   };
@@ -284,7 +283,8 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   // 32 ket rows no longer fit in L1).  Otherwise the ket side usually has more
   // primitives (s pairs against p/d pairs) and goes inside, with its next primitive
   // pair loaded one iteration ahead.
-  const R* pk0 = kprim + q;
+  // this lane's ket pair in the ket tiles: primitive ik at pkt + ik * kKetPrimStride
+  const R* __restrict__ pkt = ket_tile_ptr(ket_tiles<R>(blk.ket), q, Kcd);
   // FP32 quartets (fp32_prim_rel > 0): primitive quartets below that fraction of the
   // quartet's own Schwarz bound are skipped as well
   const R peps_r = R((F32 && args.prim_rel32 > 0.0)
@@ -293,11 +293,11 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
   if constexpr (kKetOuter) {
     const R qab_max = ib0 < Kab ? __ldg(bprim + (size_t)ib0 * nbra + p + PF_Q * sb) : R(0);
     KetPrimT<R> nxt;
-    load_ket_prim(pk0, sk, nxt);
+    load_ket_rec(pkt, nxt);
     for (int ik = 0; ik < Kcd; ++ik) {
       const KetPrimT<R> cur = nxt;
       if (qab_max * cur.q < peps_r || ib0 >= Kab) break;
-      if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
+      if (ik + 1 < Kcd) load_ket_rec(pkt + (size_t)(ik + 1) * kKetPrimStride, nxt);
       BraVals bv{};
       for (int ib = ib0; ib < Kab; ib += ibs) {
         R qab;
@@ -313,18 +313,17 @@ __device__ __forceinline__ void small_quartet(const QuartetBlock& blk, const JKA
     const R qket_max = R(blk.ket.qprim_max);
     // the first ket primitive opens every row: loaded once per quartet
     KetPrimT<R> k0;
-    load_ket_prim(pk0, sk, k0);
+    load_ket_rec(pkt, k0);
     for (int ib = ib0; ib < Kab; ib += ibs) {
       R qab;
       BraVals bv;
       load_bra(ib, qab, bv);
       if (qab * qket_max < peps_r) break;
-      KetPrimT<R> nxt;
-      nxt = k0;
+      KetPrimT<R> nxt = k0;
       for (int ik = 0; ik < Kcd; ++ik) {
         const KetPrimT<R> cur = nxt;
         if (qab * cur.q < peps_r) break;
-        if (ik + 1 < Kcd) load_ket_prim(pk0 + (size_t)(ik + 1) * nket, sk, nxt);
+        if (ik + 1 < Kcd) load_ket_rec(pkt + (size_t)(ik + 1) * kKetPrimStride, nxt);
         ++nprim_done;
         prim(bv, cur);
       }
@@ -603,14 +602,17 @@ __device__ __forceinline__ void small_finish(GV&& gval, const QuartetBlock& blk,
 // blocks, 32 warps); (ps|ss), with the first ket primitive held across its bra
 // rows, takes up to 128 without spilling (2 blocks; measured faster than 80
 // registers with spills at 3 blocks); in FP32 the one-root classes fit 64 and the
-// L = 2 ones, with their compensated accumulators, 128 (2 blocks).  The other
-// classes keep ptxas's own choice (0 = no bound; an explicit 1 would let it take
-// up to 255 registers): capping the L = 3 and 4 classes at 128 registers (2
-// blocks) measured slower in both precisions, (pp|ps) FP64 127 -> 154 ms.
+// L = 2 ones, with their compensated accumulators, 128 (2 blocks).  FP64 (dp|ss)
+// and (fs|ss) fit 128 without spilling (left free, ptxas takes 178 for (dp|ss) and
+// the class runs 19 % slower on one block).  The other classes keep ptxas's own
+// choice (0 = no bound; an explicit 1 would let it take up to 255 registers):
+// capping the other L = 3 and 4 classes at 128 registers (2 blocks) measured
+// slower in both precisions, (pp|ps) FP64 127 -> 154 ms.
 template <int LA, int LB, int LC, int LD, typename R>
 __host__ __device__ constexpr int small_min_blocks() {
   constexpr int L = LA + LB + LC + LD;
-  return sizeof(R) == 8 ? (L == 0 ? 4 : L == 1 ? 2 : 0) : (L <= 1 ? 4 : L == 2 ? 2 : 0);
+  return sizeof(R) == 8 ? (L == 0 ? 4 : L == 1 ? 2 : (LA + LB == 3 && LC + LD == 0) ? 2 : 0)
+                        : (L <= 1 ? 4 : L == 2 ? 2 : 0);
 }
 
 template <int LA, int LB, int LC, int LD, typename R, bool SPLIT>

@@ -53,6 +53,19 @@ enum BraRecField : int {
   kBraRec
 };
 
+// The same data tiled for the ket side of the thread-per-quartet kernels, whose
+// lanes read consecutive pairs: [npairs / 32 tiles][Ka*Kb][kKetRec][32], field f
+// of primitive t of pair q at ((q / 32 * Kab + t) * kKetRec + f) * 32 + q % 32.
+// A field's 32 lanes stay contiguous (coalesced, as in the SoA table), and the
+// fields and primitives of one pair are at fixed offsets from one address (no
+// per-field address arithmetic in the primitive loop).
+enum KetRecField : int {
+  KR_Q = 0, KR_ETA, KR_HE, KR_PX, KR_PY, KR_PZ, KR_QCX, KR_QCY, KR_QCZ, KR_C,
+  KR_ALPHA,  // exponent on the pair's first shell (the gradient kernels)
+  kKetRec
+};
+constexpr int kKetTile = 32;
+
 struct PairClassDev {
   int la, lb;          // la >= lb (pairs are oriented so the bra-side HRR moves to the smaller l)
   int Ka, Kb;          // nonzero primitive counts
@@ -70,6 +83,8 @@ struct PairClassDev {
   const float* primf;  // FP32 copy of prim (the FP32 kernels of mixed precision)
   const double* primb;  // [npairs][Ka*Kb][kBraRec] per-pair records (BraRecField)
   const float* primbf;  // FP32 copy of primb
+  const double* primk;  // ket tiles (KetRecField), ceil(npairs / 32) * Ka*Kb * kKetRec * 32
+  const float* primkf;  // FP32 copy of primk
 };
 
 // One launch: the canonical quartets (p, q) with p a pair of class `bra` and q a
