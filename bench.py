@@ -59,7 +59,7 @@ SYSTEMS = {
 # one timed step in a one-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum);
 # the capture and its command are summarised under profiles/.
 TRAFFIC_PER_LAUNCH = {
-    ("h2o64_ccpvdz", "(ps|ss)"): 25.52e6,  # profiles/eri_small_psss_h2o64_dram.txt
+    ("h2o64_ccpvdz", "(ps|ss)"): 25.50e6,  # profiles/eri_small_psss_h2o64_dram.txt
 }
 
 

@@ -27,7 +27,11 @@
 namespace lai {
 namespace grad_small {
 
-enum { DA = 0, DB = 1, DC = 2, DAB = 3, DABC = 4 };  // DAB: A and B in one pass; DABC: all three
+enum { DA = 0, DB = 1, DC = 2, DAB = 3, DABC = 4, DB_LO = 5, DB_HI = 6 };
+// DAB: A and B in one pass; DABC: all three.  DB_LO / DB_HI: the B pass in two halves
+// that accumulate the raised and lowered blocks only for the ket's lowest shell
+// (f = lc) / the ones above it; the gradient is linear in those blocks, so the two
+// halves add up to the B pass while each holds about half its accumulators.
 
 template <int B, int E, typename F>
 __device__ __forceinline__ void gfor(F&& f) {
@@ -78,8 +82,15 @@ constexpr int shift(int c, int x, int d) {  // component c with d added in direc
 }
 constexpr int comp_n(int c, int x) { return x == 0 ? comp_x(c) : x == 1 ? comp_y(c) : comp_z(c); }
 
-template <int LA, int LB, int LC, int LD, int DER>
+// whether a pass accumulates the raised / lowered block entries of ket shell lf
+template <int PASS, int LC>
+__host__ __device__ constexpr bool f_in_pass(int lf) {
+  return PASS == DB_LO ? lf == LC : PASS == DB_HI ? lf > LC : true;
+}
+
+template <int LA, int LB, int LC, int LD, int PASS>
 __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradSmallArgs ga, RysTablesView tab) {
+  constexpr int DER = (PASS == DB_LO || PASS == DB_HI) ? DB : PASS;
   constexpr int LAB = LA + LB, LCD = LC + LD;
   constexpr int NR = (LAB + LCD + 1) / 2 + 1;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -237,8 +248,9 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
               constexpr int jf = decltype(JF)::value;
               constexpr int lf = [] { int l = WF0, r = jf; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
               constexpr int cf = cart_comp(lf, jf - ncart_before(WF0, lf));
-              W[ie * NWF + jf] += kap2 * I[0][comp_x(ce)][comp_x(cf)] * I[1][comp_y(ce)][comp_y(cf)] *
-                                  I[2][comp_z(ce)][comp_z(cf)];
+              if constexpr (f_in_pass<PASS, LC>(lf))
+                W[ie * NWF + jf] += kap2 * I[0][comp_x(ce)][comp_x(cf)] * I[1][comp_y(ce)][comp_y(cf)] *
+                                    I[2][comp_z(ce)][comp_z(cf)];
             });
           });
           if constexpr (HAS_U) {
@@ -250,8 +262,9 @@ __global__ void __launch_bounds__(128) grad_small_kernel(QuartetBlock blk, GradS
                 constexpr int jf = decltype(JF)::value;
                 constexpr int lf = [] { int l = UF0, r = jf; while (r >= ncart(l)) { r -= ncart(l); ++l; } return l; }();
                 constexpr int cf = cart_comp(lf, jf - ncart_before(UF0, lf));
-                U[ie * NUF + jf] += I[0][comp_x(ce)][comp_x(cf)] * I[1][comp_y(ce)][comp_y(cf)] *
-                                    I[2][comp_z(ce)][comp_z(cf)];
+                if constexpr (f_in_pass<PASS, LC>(lf))
+                  U[ie * NUF + jf] += I[0][comp_x(ce)][comp_x(cf)] * I[1][comp_y(ce)][comp_y(cf)] *
+                                      I[2][comp_z(ce)][comp_z(cf)];
               });
             });
           }
@@ -414,6 +427,10 @@ int launch(const QuartetBlock& blk, const GradSmallArgs& ga, const RysTablesView
   constexpr int all_size = merged_size + ncart_range(LA, LAB) * ncart_range(LC + 1, LCD + 1) +
                            ((LC >= 1) ? ncart_range(LA, LAB) * ncart(LC - 1) : 0);
   constexpr bool kAll = all_size <= 72;
+  // a separate B pass in two halves when its raised block alone exceeds 128 doubles
+  // ((ds|pp): 144, which ptxas could only place in local memory; the halves hold 48
+  // and 96 and run about ten times faster than the whole pass)
+  constexpr bool kSplitB = ncart_range(LA, LAB + 1) * nf > 128 && LCD > LC;
   const size_t smem = table_bytes<NR, double>();
   // only the kernels this class launches are instantiated (and given their shared memory)
   auto allow = [&](auto kern) {
@@ -426,6 +443,9 @@ int launch(const QuartetBlock& blk, const GradSmallArgs& ga, const RysTablesView
       ok = allow(grad_small_kernel<LA, LB, LC, LD, DABC>);
     } else if constexpr (kMerge) {
       ok = allow(grad_small_kernel<LA, LB, LC, LD, DAB>) && allow(grad_small_kernel<LA, LB, LC, LD, DC>);
+    } else if constexpr (kSplitB) {
+      ok = allow(grad_small_kernel<LA, LB, LC, LD, DA>) && allow(grad_small_kernel<LA, LB, LC, LD, DB_LO>) &&
+           allow(grad_small_kernel<LA, LB, LC, LD, DB_HI>) && allow(grad_small_kernel<LA, LB, LC, LD, DC>);
     } else {
       ok = allow(grad_small_kernel<LA, LB, LC, LD, DA>) && allow(grad_small_kernel<LA, LB, LC, LD, DB>) &&
            allow(grad_small_kernel<LA, LB, LC, LD, DC>);
@@ -441,6 +461,10 @@ int launch(const QuartetBlock& blk, const GradSmallArgs& ga, const RysTablesView
   } else {
     if constexpr (kMerge) {
       grad_small_kernel<LA, LB, LC, LD, DAB><<<grid, threads, smem, stream>>>(blk, ga, tab);
+    } else if constexpr (kSplitB) {
+      grad_small_kernel<LA, LB, LC, LD, DA><<<grid, threads, smem, stream>>>(blk, ga, tab);
+      grad_small_kernel<LA, LB, LC, LD, DB_LO><<<grid, threads, smem, stream>>>(blk, ga, tab);
+      grad_small_kernel<LA, LB, LC, LD, DB_HI><<<grid, threads, smem, stream>>>(blk, ga, tab);
     } else {
       grad_small_kernel<LA, LB, LC, LD, DA><<<grid, threads, smem, stream>>>(blk, ga, tab);
       grad_small_kernel<LA, LB, LC, LD, DB><<<grid, threads, smem, stream>>>(blk, ga, tab);
