@@ -429,7 +429,10 @@ int launch(const QuartetBlock& blk, const GradSmallArgs& ga, const RysTablesView
   constexpr bool kAll = all_size <= 72;
   // a separate B pass in two halves when its raised block alone exceeds 128 doubles
   // ((ds|pp): 144, which ptxas could only place in local memory; the halves hold 48
-  // and 96 and run about ten times faster than the whole pass)
+  // and 96 and run about ten times faster than the whole pass).  Halving the other
+  // passes that spill a little ((ds|pp) A and C, (dp|ps), (ds|ds), (dd|ss): 0.5-2.3 KB
+  // per thread) measured 9-43 % slower per class: the second primitive loop costs
+  // more than those spills.
   constexpr bool kSplitB = ncart_range(LA, LAB + 1) * nf > 128 && LCD > LC;
   const size_t smem = table_bytes<NR, double>();
   // only the kernels this class launches are instantiated (and given their shared memory)

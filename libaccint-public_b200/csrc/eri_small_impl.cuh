@@ -599,7 +599,8 @@ __device__ __forceinline__ void small_finish(GV&& gval, const QuartetBlock& blk,
 // Blocks per SM the register allocation must allow (ptxas caps registers at
 // 65536 / (256 * blocks)).  The light classes are latency bound with short
 // dependent chains and need the warps: in FP64 (ss|ss) fits 64 registers (4
-// blocks, 32 warps); (ps|ss), with the first ket primitive held across its bra
+// blocks, 32 warps; at 3 blocks it takes 72 without spilling and runs 1-2 % slower);
+// (ps|ss), with the first ket primitive held across its bra
 // rows, takes up to 128 without spilling (2 blocks; measured faster than 80
 // registers with spills at 3 blocks); in FP32 the one-root classes fit 64 and the
 // L = 2 ones, with their compensated accumulators, 128 (2 blocks).  FP64 (dp|ss)
