@@ -2,7 +2,8 @@
 // (the (e0|f0) block of one quartet is too large for one thread's registers,
 // e.g. (dp|pp), (dp|dp), (dd|ps), (dd|ds)).
 //
-// A group of TW = next_pow2(na) lanes works on one quartet; lane a of the group
+// A group of TW = na lanes works on one quartet (32 / na groups per warp, the
+// remaining 32 mod na lanes idle); lane a of the group
 // owns Cartesian component a of the bra's first shell.  Every lane evaluates the
 // roots and the full 2D tables of each primitive quartet (cheap next to the
 // assembly for these classes), then accumulates only the rows of (e0|f0) its
@@ -10,7 +11,7 @@
 // until digestion.  Lane a then forms its outputs (a b|c d) for all b, c, d by
 // the closed-form transfer (eri_device.cuh) and digests them:
 //   J_ij[a][b], K_ik[a][c], K_il[a][d]   complete in the lane -> atomics;
-//   J_kl, K_jk, K_jl                      partial over a -> butterfly sum over
+//   J_kl, K_jk, K_jl                      partial over a -> shuffle sum over
 //                                         the group, then one atomic per entry.
 // The lane-dependent row offset a is applied by selecting rows of the 2D tables
 // (compile-time-indexed registers) instead of indexing them at run time.
@@ -41,6 +42,23 @@ __host__ __device__ constexpr int next_pow2(int x) {
   return p;
 }
 
+// Reduction over the TW lanes g*TW .. g*TW+TW-1 of a group (TW need not be a power of
+// two) into the group's lane a == 0 (the other lanes' results are partial): the lanes
+// past the largest power of two P < TW fold onto the first ones, then a halving tree.
+template <int TW, typename T, typename Op>
+__device__ __forceinline__ T group_reduce(T v, int a, Op op) {
+  constexpr int P = next_pow2(TW) == TW ? TW / 2 : next_pow2(TW) / 2;
+  if constexpr (P * 2 > TW) {
+    const T u = __shfl_down_sync(0xffffffffu, v, P);
+    if (a + P < TW) v = op(v, u);
+  } else {
+    v = op(v, __shfl_down_sync(0xffffffffu, v, P));
+  }
+#pragma unroll
+  for (int o = P / 2; o > 0; o >>= 1) v = op(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JKArgs& args,
                                                const RysTablesView& tab,
@@ -51,7 +69,7 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr int NF = ncart_range(LC, LCD);
   constexpr int NK = ncart_range(0, LB);  // shifts k with |k| <= lb
-  constexpr int TW = next_pow2(NA);
+  constexpr int TW = NA;
   constexpr int W = LCD + 1;
   const int nbra = blk.bra.npairs, nket = blk.ket.npairs;
   const int q = (blk.qbegin ? __ldg(blk.qbegin + p) : 0) + (int)(t - __ldg(blk.offsets + p));
@@ -267,8 +285,7 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 #pragma unroll
           for (int b = 0; b < NB; ++b) mx = fmax(mx, fabs(V[(b * NC + c) * ND + b]));
     }
-#pragma unroll
-    for (int o = TW / 2; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o, TW));
+    mx = group_reduce<TW>(mx, a, [](double x, double y) { return fmax(x, y); });
     if (active && a == 0) args.schwarz_out[p] = sqrt(mx);
     return;
   }
@@ -327,7 +344,7 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
       if (own) atomicAdd(K + (size_t)arow * nbf + fd + d, sym * v);
     }
   }
-  // partial-over-a targets: group butterfly sum, then lane (i % TW) does entry i
+  // partial-over-a targets: group sum into lane a == 0, which does the atomics
   {  // J_kl[c][d] = 2 s sum_a sum_b V D_ij[a][b]
     double Di[NB];
 #pragma unroll
@@ -338,9 +355,8 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 #pragma unroll
       for (int b = 0; b < NB; ++b) v += V[b * NC * ND + cd] * Di[b];
       v *= 2.0 * sym;
-#pragma unroll
-      for (int o = TW / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, TW);
-      if (active && (cd % TW) == (a & (TW - 1)))
+      v = group_reduce<TW>(v, a, [](double x, double y) { return x + y; });
+      if (active && a == 0)
         atomicAdd(J + (size_t)(fc + cd / ND) * nbf + fd + cd % ND, v);
     }
   }
@@ -354,9 +370,8 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 #pragma unroll
       for (int d = 0; d < ND; ++d) v += V[bc * ND + d] * Dl[d];
       v *= sym;
-#pragma unroll
-      for (int o = TW / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, TW);
-      if (active && (bc % TW) == (a & (TW - 1)))
+      v = group_reduce<TW>(v, a, [](double x, double y) { return x + y; });
+      if (active && a == 0)
         atomicAdd(K + (size_t)(fb + bc / NC) * nbf + fc + bc % NC, v);
     }
   }
@@ -371,9 +386,8 @@ __device__ __forceinline__ void sliced_quartet(const QuartetBlock& blk, const JK
 #pragma unroll
       for (int c = 0; c < NC; ++c) v += V[(b * NC + c) * ND + d] * Dc[c];
       v *= sym;
-#pragma unroll
-      for (int o = TW / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, TW);
-      if (active && (bd % TW) == (a & (TW - 1)))
+      v = group_reduce<TW>(v, a, [](double x, double y) { return x + y; });
+      if (active && a == 0)
         atomicAdd(K + (size_t)(fb + b) * nbf + fd + d, v);
     }
   }
@@ -383,8 +397,8 @@ template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) eri_sliced_kernel(QuartetBlock blk, JKArgs args,
                                                          RysTablesView tab, int kSuper) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
-  constexpr int TW = next_pow2(ncart(LA));
-  constexpr int QPW = 32 / TW;  // quartets per warp
+  constexpr int TW = ncart(LA);
+  constexpr int QPW = 32 / TW;  // quartets per warp (lanes QPW * TW .. 31 idle)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* stab = reinterpret_cast<R*>(smem_raw);
   stage_table<NR, R>(stab, tab);
@@ -403,8 +417,10 @@ __global__ void __launch_bounds__(128) eri_sliced_kernel(QuartetBlock blk, JKArg
     for (int64_t c = sc * kSuper; c < c1; ++c) {
       const int64_t t0 = blk.t_begin + c * QPW;
       const int64_t t = t0 + slot;
-      const bool active = t < blk.total;
-      const int64_t te = active ? t : blk.total - 1;
+      const bool active = slot < QPW && t < blk.total;
+      // idle lanes take the chunk's first quartet (t0 < total), whose bra pair the
+      // warp already holds
+      const int64_t te = active ? t : t0;
       if (pw < 0) {
         if (lane == 0) pw = find_bra(blk.offsets, nbra, t0);
         pw = __shfl_sync(0xffffffffu, pw, 0);
@@ -422,7 +438,7 @@ template <int LA, int LB, int LC, int LD>
 int launch_one(const QuartetBlock& blk, const JKArgs& args, const RysTablesView& tab,
                cudaStream_t stream, bool fp32, int num_sms) {
   constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
-  constexpr int QPW = 32 / next_pow2(ncart(LA));
+  constexpr int QPW = 32 / ncart(LA);
   const int threads = 128;
   const size_t smem = fp32 ? table_bytes<NR, float>() : table_bytes<NR, double>();
   const int64_t nchunks = (blk.total - blk.t_begin + QPW - 1) / QPW;
